@@ -1,0 +1,111 @@
+// Per-arena working state of one simulation tick.
+//
+// The tick is a restatement of RocketSim's Arena::Step (Arena.cpp:716-812) over Bullet's
+// btDiscreteDynamicsWorld::stepSimulation (btDiscreteDynamicsWorld.cpp:320-437).  Object
+// numbering follows the reference's collision-object array, which fixes the order of
+// broadphase pairs, manifolds and solver rows:
+//   0..15  arena meshes (soccar/mesh_0..15)       static, friction 0.6, restitution 0.3
+//   16..19 planes: floor, ceiling, -x wall, +x wall  static, same material
+//   20     ball
+//   21..26 cars, blue first then orange (Arena::AddCar order)
+#pragma once
+#include "arena_static.h"
+#include "consts.h"
+
+namespace rsb {
+
+constexpr int OBJ_BALL = NUM_STATICS;       // 20
+constexpr int OBJ_CAR0 = NUM_STATICS + 1;   // 21
+constexpr int MAX_CARS = 6;
+constexpr int MAX_BODIES = 1 + MAX_CARS;
+
+// btCollisionObject activation states (btCollisionObject.h)
+enum : int32_t { ACT_ACTIVE = 1, ACT_SLEEPING = 2, ACT_WANTS_DEACT = 3, ACT_DISABLE_DEACT = 4, ACT_DISABLE_SIM = 5 };
+
+constexpr float STATIC_FRICTION = 0.6f, STATIC_RESTITUTION = 0.3f;
+
+struct Body {
+    Xf xf;       // world transform (Bullet units)
+    Xf ixf;      // interpolation transform = this tick's predicted transform
+    V3 lin, ang; // velocities
+    V3 force, torque;
+    M3 invIw;    // m_invInertiaTensorWorld
+    V3 invIl;    // m_invInertiaLocal
+    float invMass;
+    V3 grav;     // m_gravity (force)
+    float linDampFactor;  // btPow(1 - linearDamping, dt), precomputed on the host
+    float friction, restitution;
+    int32_t act;
+    int32_t noResp;       // CF_NO_CONTACT_RESPONSE
+    int32_t islandTag;
+    int32_t solverId;
+    // broadphase proxy
+    V3 bpMin, bpMax;
+    int32_t cell, ci, cj, ck;
+    int32_t regStamp;     // order of the last (re-)registration in the grid cells
+    // special-contact aggregation (btCollisionObject::m_specialResolveInfo)
+    int32_t spCount;
+    float spFric, spRest, spDist;
+    V3 spNormal;
+};
+
+// btManifoldPoint fields the pipeline uses
+struct MPoint {
+    V3 localA, localB, posA, posB, normal;
+    float dist, fric, rest;
+    int32_t index1;   // triangle index on the B side (-1 when B is not a mesh)
+    int32_t special;
+};
+
+constexpr int MAX_MANIFOLDS = 48;
+constexpr int MAX_POINTS = 4;
+
+struct Manifold {
+    int32_t o0, o1;   // object ids (body0 / body1)
+    float cbt;        // contact breaking threshold
+    int32_t n;
+    MPoint pt[MAX_POINTS];
+};
+
+// btSolverConstraint fields used by contact and friction rows
+struct SRow {
+    V3 n1, rc1, angA;  // m_contactNormal1, m_relpos1CrossNormal, m_angularComponentA
+    V3 n2, rc2, angB;
+    float rhs, rhsPen, cfm, jacInv, lo, hi, friction;
+    float applied, appliedPush;
+    int16_t bA, bB;   // solver body ids
+    int16_t fIdx;     // contact row: first friction row; friction row: its contact row
+    int16_t special;
+};
+
+struct SBody {
+    Xf xf;
+    V3 invMassV;
+    V3 lin, ang;       // velocities at solve start
+    V3 extF, extT;     // m_externalForceImpulse / m_externalTorqueImpulse
+    V3 dLin, dAng;     // delta velocities
+    V3 push, turn;
+    int32_t body;      // index into Arena.bodies, -1 for the fixed body
+};
+
+constexpr int MAX_CONTACT_ROWS = 64;
+constexpr int MAX_FRICTION_ROWS = 64;
+constexpr int MAX_PAIRS = 64;
+
+struct WorldParams {
+    float dt;                 // 1/120
+    V3 gravity;               // Bullet units
+    float ballLinDampFactor;  // btPow(1 - ballDrag, dt)
+    float ballRadius;         // Bullet units
+    float ballMargin;         // sphere margin (= radius)
+    float ballAabbExt;        // margin + 0.08f
+    float ballCbt;            // contact breaking threshold of the ball shape
+    float ballInvMass;
+    V3 ballGrav;
+    V3 ballInvInertia;
+    float ballFriction, ballRestitution;
+    float ballMaxSpeedBt;
+    int32_t numDynProxiesExtra; // unused, keeps layout stable
+};
+
+}  // namespace rsb

@@ -1,0 +1,382 @@
+"""Python binding of the engine's C ABI (include/rsb.h).
+
+The same binding drives any library that exports the rsb_* symbols: the CUDA
+engine (``librsb.so`` in this package) and, in tests and the CPU-baseline leg of
+the benchmark, the reference-backed oracle library.  Bulk state I/O goes through
+numpy structured arrays whose dtypes mirror the C structs byte for byte.
+
+The class mirrors the reference batch simulator's public methods
+(RocketSimCuda/include/RocketSimCuda.h:258-396): ``create`` ~ Init + AddCar,
+``reset_all`` ~ ResetAllArenas, ``set_actions`` ~ SetDiscreteActionsFromIndices,
+``step`` ~ Step, ``build_obs`` ~ BuildAdvancedObsAndDefaultMasks,
+``build_rewards_terminals`` ~ BuildRewardsAndTerminals, ``get_cars`` ~
+GetAllCarStates and so on.  Errors raise :class:`RsbError` with the library's
+message instead of being printed and ignored.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+RSB_MAX_CARS_PER_ARENA = 6
+RSB_NUM_PADS = 34
+RSB_NUM_ACTIONS = 90
+RSB_OBS_BASE = 51
+RSB_OBS_PER_CAR = 29
+
+RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS = range(6)
+RSB_CULL_EXACT, RSB_CULL_LEARNED = 0, 1
+RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT = 0, 1, 2
+
+_STATUS = {
+    -1: "RSB_ERR_INVALID", -2: "RSB_ERR_CUDA", -3: "RSB_ERR_NOMEM", -4: "RSB_ERR_MESH",
+    -5: "RSB_ERR_STATE", -6: "RSB_ERR_TIMEOUT", -7: "RSB_ERR_UNSUPPORTED",
+}
+
+
+class RsbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class RotMat(C.Structure):
+    _fields_ = [("forward", Vec3), ("right", Vec3), ("up", Vec3)]
+
+
+class Controls(C.Structure):
+    _fields_ = [("throttle", C.c_float), ("steer", C.c_float), ("pitch", C.c_float),
+                ("yaw", C.c_float), ("roll", C.c_float), ("jump", C.c_uint8),
+                ("boost", C.c_uint8), ("handbrake", C.c_uint8), ("pad_", C.c_uint8)]
+
+
+class CarState(C.Structure):
+    _fields_ = [
+        ("pos", Vec3), ("rot", RotMat), ("vel", Vec3), ("ang_vel", Vec3),
+        ("boost", C.c_float), ("time_spent_boosting", C.c_float),
+        ("jump_time", C.c_float), ("flip_time", C.c_float), ("air_time", C.c_float),
+        ("air_time_since_jump", C.c_float), ("supersonic_time", C.c_float),
+        ("handbrake_val", C.c_float), ("auto_flip_timer", C.c_float),
+        ("auto_flip_torque_scale", C.c_float), ("demo_respawn_timer", C.c_float),
+        ("car_contact_cooldown", C.c_float), ("flip_rel_torque", Vec3),
+        ("world_contact_normal", Vec3), ("car_contact_other_id", C.c_uint32),
+        ("is_on_ground", C.c_uint8), ("has_jumped", C.c_uint8), ("has_double_jumped", C.c_uint8),
+        ("has_flipped", C.c_uint8), ("is_flipping", C.c_uint8), ("is_jumping", C.c_uint8),
+        ("is_supersonic", C.c_uint8), ("is_auto_flipping", C.c_uint8), ("is_demoed", C.c_uint8),
+        ("world_contact", C.c_uint8), ("ball_hit_valid", C.c_uint8), ("team", C.c_uint8),
+        ("wheels_with_contact", C.c_uint8 * 4),
+        ("ball_hit_tick", C.c_uint64), ("ball_hit_extra_tick", C.c_uint64),
+        ("ball_hit_rel_pos", Vec3), ("ball_hit_ball_pos", Vec3), ("ball_hit_extra_vel", Vec3),
+        ("last_controls", Controls), ("id", C.c_uint32), ("pad_", C.c_uint32),
+    ]
+
+
+class BallState(C.Structure):
+    _fields_ = [("pos", Vec3), ("rot", RotMat), ("vel", Vec3), ("ang_vel", Vec3)]
+
+
+class PadState(C.Structure):
+    _fields_ = [("is_active", C.c_uint8), ("pad_", C.c_uint8 * 3), ("cooldown", C.c_float),
+                ("prev_locked_car_id", C.c_uint32)]
+
+
+class ArenaInfo(C.Structure):
+    _fields_ = [("tick_count", C.c_uint64), ("num_cars", C.c_int32), ("team_size", C.c_int32),
+                ("goal_scored", C.c_int32), ("goal_team", C.c_int32),
+                ("episode_ticks", C.c_int32), ("status", C.c_int32)]
+
+
+class Mutators(C.Structure):
+    _fields_ = [("gravity", Vec3)] + [(n, C.c_float) for n in (
+        "car_mass", "car_world_friction", "car_world_restitution", "ball_mass", "ball_max_speed",
+        "ball_drag", "ball_world_friction", "ball_world_restitution", "jump_accel",
+        "jump_immediate_force", "boost_accel_ground", "boost_accel_air", "boost_used_per_second",
+        "respawn_delay", "bump_cooldown_time", "boost_pad_cooldown_big", "boost_pad_cooldown_small",
+        "car_spawn_boost_amount", "ball_hit_extra_force_scale", "bump_force_scale", "ball_radius")] + [
+        ("unlimited_flips", C.c_uint8), ("unlimited_double_jumps", C.c_uint8),
+        ("demo_mode", C.c_uint8), ("enable_team_demos", C.c_uint8),
+        ("goal_base_threshold_y", C.c_float)]
+
+
+class RewardConfig(C.Structure):
+    _fields_ = [("w_goal", C.c_float), ("w_touch", C.c_float), ("w_vel_ball_to_goal", C.c_float),
+                ("w_vel_player_to_ball", C.c_float), ("goal_concede_scale", C.c_float),
+                ("team_spirit", C.c_float), ("opponent_scale", C.c_float), ("zero_sum", C.c_int32),
+                ("episode_max_ticks", C.c_int32), ("no_touch_timeout_s", C.c_float)]
+
+
+class Config(C.Structure):
+    _fields_ = [("num_arenas", C.c_int32), ("team_size", C.c_int32),
+                ("team_sizes", C.POINTER(C.c_int32)), ("tick_rate", C.c_float),
+                ("tick_skip", C.c_int32), ("meshes_path", C.c_char_p),
+                ("mutators", C.POINTER(Mutators)), ("rewards", C.POINTER(RewardConfig)),
+                ("cull_mode", C.c_int32), ("cull_margin", C.c_float), ("seed", C.c_uint64),
+                ("device", C.c_int32), ("threads", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "ticks_simulated", "narrowphase_queries", "culled_queries", "missed_contacts",
+        "solver_rows", "arenas_reverted", "status_bits_seen")]
+
+
+CAR_DTYPE = np.dtype(CarState)
+BALL_DTYPE = np.dtype(BallState)
+PAD_DTYPE = np.dtype(PadState)
+INFO_DTYPE = np.dtype(ArenaInfo)
+CONTROLS_DTYPE = np.dtype(Controls)
+
+_P = C.c_void_p
+_SIGS = {
+    "rsb_default_mutators": [C.POINTER(Mutators)],
+    "rsb_default_rewards": [C.POINTER(RewardConfig)],
+    "rsb_create": [C.POINTER(Config), C.POINTER(_P)],
+    "rsb_destroy": [_P],
+    "rsb_layout": [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _P, _P],
+    "rsb_obs_stride": [_P, C.POINTER(C.c_int32)],
+    "rsb_reset_all": [_P, C.c_uint64, C.c_int32],
+    "rsb_reset_arenas": [_P, _P, C.c_int32, C.c_uint64, C.c_int32],
+    "rsb_set_action_lut": [_P, _P, C.c_int32],
+    "rsb_default_action_lut": [_P, C.c_int32],
+    "rsb_set_actions_host": [_P, _P, C.c_int32],
+    "rsb_set_actions_device": [_P, _P, C.c_int32, _P],
+    "rsb_set_controls": [_P, _P, C.c_int32],
+    "rsb_step": [_P, C.c_int32, _P],
+    "rsb_snapshot": [_P, _P],
+    "rsb_build_obs": [_P, _P],
+    "rsb_build_rewards_terminals": [_P, C.c_int32, _P],
+    "rsb_copy_obs": [_P, _P, C.c_size_t],
+    "rsb_copy_masks": [_P, _P, C.c_size_t],
+    "rsb_copy_rewards": [_P, _P, C.c_size_t],
+    "rsb_copy_terminals": [_P, _P, C.c_size_t],
+    "rsb_device_ptr": [_P, C.c_int32, C.POINTER(_P)],
+    "rsb_get_cars": [_P, _P, C.c_int32],
+    "rsb_set_cars": [_P, _P, C.c_int32],
+    "rsb_get_balls": [_P, _P, C.c_int32],
+    "rsb_set_balls": [_P, _P, C.c_int32],
+    "rsb_get_pads": [_P, _P, C.c_int32],
+    "rsb_set_pads": [_P, _P, C.c_int32],
+    "rsb_get_arena_info": [_P, _P, C.c_int32],
+    "rsb_sync": [_P],
+    "rsb_stats_get": [_P, C.POINTER(Stats)],
+    "rsb_last_error": [_P, C.c_char_p, C.c_size_t],
+}
+
+#: every symbol include/rsb.h declares (checked by the ABI tests)
+ABI_SYMBOLS = tuple(_SIGS.keys())
+
+_LIBS: dict[str, C.CDLL] = {}
+
+
+def load_library(path: str) -> C.CDLL:
+    """Loads (once) a library exporting the rsb_* ABI and declares its signatures."""
+    path = os.path.abspath(path)
+    if path in _LIBS:
+        return _LIBS[path]
+    lib = C.CDLL(path, mode=C.RTLD_GLOBAL)
+    for name, args in _SIGS.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.argtypes = args
+        fn.restype = C.c_int32
+    _LIBS[path] = lib
+    return lib
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def default_mutators(lib: C.CDLL) -> Mutators:
+    m = Mutators()
+    lib.rsb_default_mutators(C.byref(m))
+    return m
+
+
+def default_action_lut(lib: C.CDLL) -> np.ndarray:
+    lut = np.zeros(RSB_NUM_ACTIONS, CONTROLS_DTYPE)
+    st = lib.rsb_default_action_lut(_ptr(lut), RSB_NUM_ACTIONS)
+    if st != 0:
+        raise RsbError(st, "rsb_default_action_lut failed")
+    return lut
+
+
+class Batch:
+    """N arenas behind one rsb handle."""
+
+    def __init__(self, lib: C.CDLL | str, num_arenas: int, team_size: int | None = 2,
+                 team_sizes=None, meshes_path: str = "", tick_skip: int = 8,
+                 mutators: Mutators | None = None, rewards: RewardConfig | None = None,
+                 cull_mode: int = RSB_CULL_EXACT, cull_margin: float = 0.0, seed: int = 0,
+                 device: int = 0, threads: int = 0):
+        self.lib = load_library(lib) if isinstance(lib, str) else lib
+        self._h = C.c_void_p()
+        cfg = Config()
+        cfg.num_arenas = num_arenas
+        cfg.team_size = team_size or 0
+        self._team_sizes = None
+        if team_sizes is not None:
+            self._team_sizes = np.ascontiguousarray(team_sizes, np.int32)
+            cfg.team_sizes = self._team_sizes.ctypes.data_as(C.POINTER(C.c_int32))
+        cfg.tick_rate = 120.0
+        cfg.tick_skip = tick_skip
+        cfg.meshes_path = meshes_path.encode()
+        self._mut = mutators
+        if mutators is not None:
+            cfg.mutators = C.pointer(mutators)
+        self._rew = rewards
+        if rewards is not None:
+            cfg.rewards = C.pointer(rewards)
+        cfg.cull_mode = cull_mode
+        cfg.cull_margin = cull_margin
+        cfg.seed = seed
+        cfg.device = device
+        cfg.threads = threads
+        st = self.lib.rsb_create(C.byref(cfg), C.byref(self._h))
+        if st != 0:
+            raise RsbError(st, self._error(None))
+        na, nc = C.c_int32(), C.c_int32()
+        self._check(self.lib.rsb_layout(self._h, C.byref(na), C.byref(nc), None, None))
+        self.num_arenas, self.num_cars = na.value, nc.value
+        self.car_offset = np.zeros(self.num_arenas + 1, np.int32)
+        self.team_size = np.zeros(self.num_arenas, np.int32)
+        self._check(self.lib.rsb_layout(self._h, None, None, _ptr(self.car_offset), _ptr(self.team_size)))
+        stride = C.c_int32()
+        self._check(self.lib.rsb_obs_stride(self._h, C.byref(stride)))
+        self.obs_stride = stride.value
+
+    # ---------------------------------------------------------------- plumbing
+    def _error(self, h) -> str:
+        buf = C.create_string_buffer(512)
+        self.lib.rsb_last_error(h, buf, 512)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, st: int):
+        if st != 0:
+            raise RsbError(st, self._error(self._h))
+
+    def close(self):
+        if self._h:
+            self.lib.rsb_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---------------------------------------------------------------- control
+    def reset_all(self, seed: int, mode: int = RSB_RESET_KICKOFF):
+        self._check(self.lib.rsb_reset_all(self._h, seed, mode))
+
+    def reset_arenas(self, idx, seed: int, mode: int = RSB_RESET_KICKOFF):
+        a = np.ascontiguousarray(idx, np.int32)
+        self._check(self.lib.rsb_reset_arenas(self._h, _ptr(a), len(a), seed, mode))
+
+    def set_action_lut(self, lut: np.ndarray):
+        lut = np.ascontiguousarray(lut, CONTROLS_DTYPE)
+        self._check(self.lib.rsb_set_action_lut(self._h, _ptr(lut), len(lut)))
+
+    def set_actions(self, idx):
+        a = np.ascontiguousarray(idx, np.int32)
+        self._check(self.lib.rsb_set_actions_host(self._h, _ptr(a), len(a)))
+
+    def set_actions_device(self, dev_ptr: int, n: int, stream: int | None = None):
+        self._check(self.lib.rsb_set_actions_device(self._h, C.c_void_p(dev_ptr), n, C.c_void_p(stream or 0)))
+
+    def set_controls(self, controls: np.ndarray):
+        c = np.ascontiguousarray(controls, CONTROLS_DTYPE)
+        self._check(self.lib.rsb_set_controls(self._h, _ptr(c), len(c)))
+
+    def step(self, ticks: int, stream: int | None = None):
+        self._check(self.lib.rsb_step(self._h, ticks, C.c_void_p(stream or 0)))
+
+    def snapshot(self, stream: int | None = None):
+        self._check(self.lib.rsb_snapshot(self._h, C.c_void_p(stream or 0)))
+
+    def build_obs(self, stream: int | None = None):
+        self._check(self.lib.rsb_build_obs(self._h, C.c_void_p(stream or 0)))
+
+    def build_rewards_terminals(self, step_ticks: int, stream: int | None = None):
+        self._check(self.lib.rsb_build_rewards_terminals(self._h, step_ticks, C.c_void_p(stream or 0)))
+
+    def sync(self):
+        self._check(self.lib.rsb_sync(self._h))
+
+    # ---------------------------------------------------------------- buffers
+    def copy_obs(self) -> np.ndarray:
+        out = np.zeros((self.num_cars, self.obs_stride), np.float32)
+        self._check(self.lib.rsb_copy_obs(self._h, _ptr(out), out.size))
+        return out
+
+    def copy_masks(self) -> np.ndarray:
+        out = np.zeros((self.num_cars, RSB_NUM_ACTIONS), np.uint8)
+        self._check(self.lib.rsb_copy_masks(self._h, _ptr(out), out.size))
+        return out
+
+    def copy_rewards(self) -> np.ndarray:
+        out = np.zeros(self.num_cars, np.float32)
+        self._check(self.lib.rsb_copy_rewards(self._h, _ptr(out), out.size))
+        return out
+
+    def copy_terminals(self) -> np.ndarray:
+        out = np.zeros(self.num_arenas, np.uint8)
+        self._check(self.lib.rsb_copy_terminals(self._h, _ptr(out), out.size))
+        return out
+
+    def device_ptr(self, which: int) -> int:
+        p = C.c_void_p()
+        self._check(self.lib.rsb_device_ptr(self._h, which, C.byref(p)))
+        return p.value or 0
+
+    # ---------------------------------------------------------------- state
+    def get_cars(self) -> np.ndarray:
+        out = np.zeros(self.num_cars, CAR_DTYPE)
+        self._check(self.lib.rsb_get_cars(self._h, _ptr(out), self.num_cars))
+        return out
+
+    def set_cars(self, cars: np.ndarray):
+        c = np.ascontiguousarray(cars, CAR_DTYPE)
+        self._check(self.lib.rsb_set_cars(self._h, _ptr(c), len(c)))
+
+    def get_balls(self) -> np.ndarray:
+        out = np.zeros(self.num_arenas, BALL_DTYPE)
+        self._check(self.lib.rsb_get_balls(self._h, _ptr(out), self.num_arenas))
+        return out
+
+    def set_balls(self, balls: np.ndarray):
+        b = np.ascontiguousarray(balls, BALL_DTYPE)
+        self._check(self.lib.rsb_set_balls(self._h, _ptr(b), len(b)))
+
+    def get_pads(self) -> np.ndarray:
+        out = np.zeros(self.num_arenas * RSB_NUM_PADS, PAD_DTYPE)
+        self._check(self.lib.rsb_get_pads(self._h, _ptr(out), len(out)))
+        return out
+
+    def set_pads(self, pads: np.ndarray):
+        p = np.ascontiguousarray(pads, PAD_DTYPE)
+        self._check(self.lib.rsb_set_pads(self._h, _ptr(p), len(p)))
+
+    def get_arena_info(self) -> np.ndarray:
+        out = np.zeros(self.num_arenas, INFO_DTYPE)
+        self._check(self.lib.rsb_get_arena_info(self._h, _ptr(out), self.num_arenas))
+        return out
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self.lib.rsb_stats_get(self._h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in Stats._fields_}

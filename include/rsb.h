@@ -1,0 +1,283 @@
+/*
+ * rsb.h — C ABI of the batched RocketSim engine for B200 (sm_100a).
+ *
+ * One handle owns N independent soccar arenas (ragged 1v1 / 2v2 / 3v3) whose
+ * whole state lives in device memory.  The entry points mirror the public
+ * methods of the reference batch simulator so that the PPO collector's env
+ * layer can switch to this library without changing its call sequence:
+ *
+ *   reference (RocketSimCuda/include/RocketSimCuda.h)      this ABI
+ *   -----------------------------------------------------  ------------------------------
+ *   RocketSimCudaBatch::Init            :264               rsb_create
+ *   RocketSimCudaBatch::Destroy         :267               rsb_destroy
+ *   RocketSimCudaBatch::AddCar          :272               rsb_config.team_sizes (cars are
+ *                                                          laid out blue first, then orange)
+ *   RocketSimCudaBatch::ResetArena      :275               rsb_reset_arenas
+ *   RocketSimCudaBatch::ResetAllArenas  :278               rsb_reset_all
+ *   RocketSimCudaBatch::UploadDiscreteActionLut :293       rsb_set_action_lut
+ *   RocketSimCudaBatch::SetDiscreteActionsFromIndices :297 rsb_set_actions_host
+ *   RocketSimCudaBatch::SetDiscreteActionsFromDevice  :300 rsb_set_actions_device
+ *   RocketSimCudaBatch::SetAllCarControls :290             rsb_set_controls
+ *   RocketSimCudaBatch::Step            :310               rsb_step
+ *   RocketSimCudaBatch::BuildAdvancedObsAndDefaultMasks :316 rsb_build_obs
+ *   RocketSimCudaBatch::SnapshotTrainingState :334         rsb_snapshot
+ *   RocketSimCudaBatch::BuildRewardsAndTerminals :339      rsb_build_rewards_terminals
+ *   RocketSimCudaBatch::CopyBuilt*      :342-345           rsb_copy_obs / _masks / _rewards / _terminals
+ *   RocketSimCudaBatch::Get*DevicePtr   :387-396           rsb_device_ptr
+ *   RocketSimCudaBatch::GetAllCarStates :355               rsb_get_cars
+ *   RocketSimCudaBatch::GetAllBallStates :361              rsb_get_balls
+ *   RocketSimCudaBatch::GetAllBoostPadStates :365          rsb_get_pads
+ *   RocketSimCudaBatch::GetAllArenaInfos :369              rsb_get_arena_info
+ *   RocketSimCudaBatch::SetCarState/SetBallState/SetAllBoostPadStates :377-383
+ *                                                          rsb_set_cars / rsb_set_balls / rsb_set_pads
+ *   RocketSimCudaBatch::Synchronize     :346               rsb_sync
+ *   (none: errors were printed and ignored)                rsb_last_error, rsb_stats
+ *
+ * Conventions
+ *   - Every function returns an rsb_status (0 = ok).  On error the handle keeps a
+ *     message that rsb_last_error() returns.  Nothing is printed.
+ *   - Units are Unreal units (uu) and seconds, as in RocketSim's public states.
+ *   - "stream" arguments are a cudaStream_t passed as void*; NULL = the handle's
+ *     own stream.  Host-buffer functions synchronise that stream before returning.
+ *   - Car c of arena a is global car index car_offset[a] + c.  Within an arena the
+ *     first team_size cars are blue, the next team_size orange.  Car ids (used by
+ *     boost-pad locks and bump cooldowns) are c + 1, as RocketSim's Arena::AddCar
+ *     assigns them in that order.
+ *   - Boost pads use RocketSim's arena order (6 big pads first, then 28 small).
+ */
+#ifndef RSB_H
+#define RSB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RSB_MAX_TEAM_SIZE 3
+#define RSB_MAX_CARS_PER_ARENA 6
+#define RSB_NUM_PADS 34
+#define RSB_NUM_ACTIONS 90
+#define RSB_OBS_BASE 51
+#define RSB_OBS_PER_CAR 29
+
+typedef int32_t rsb_status;
+enum {
+    RSB_OK = 0,
+    RSB_ERR_INVALID = -1,     /* bad argument or size */
+    RSB_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    RSB_ERR_NOMEM = -3,       /* allocation failed */
+    RSB_ERR_MESH = -4,        /* collision meshes missing or malformed */
+    RSB_ERR_STATE = -5,       /* call out of order (e.g. no action table) */
+    RSB_ERR_TIMEOUT = -6,     /* a bounded device wait ran out */
+    RSB_ERR_UNSUPPORTED = -7  /* option not built into this library */
+};
+
+/* Which device buffer rsb_device_ptr returns. */
+enum {
+    RSB_BUF_OBS = 0,        /* float [num_cars][obs_stride] */
+    RSB_BUF_MASKS = 1,      /* uint8 [num_cars][90] */
+    RSB_BUF_REWARDS = 2,    /* float [num_cars] */
+    RSB_BUF_TERMINALS = 3,  /* uint8 [num_arenas]: 0 none, 1 goal, 2 timeout */
+    RSB_BUF_CONTROLS = 4,   /* rsb_controls [num_cars] */
+    RSB_BUF_ACTIONS = 5     /* int32 [num_cars] */
+};
+
+/* Arena-narrowphase mode. */
+enum {
+    RSB_CULL_EXACT = 0,   /* every query runs the exact BVH narrowphase */
+    RSB_CULL_LEARNED = 1  /* a learned distance bound skips queries that are provably clear */
+};
+
+/* Reset modes for rsb_reset_arenas. */
+enum {
+    RSB_RESET_KICKOFF = 0,      /* RocketSim Arena::ResetToRandomKickoff layout */
+    RSB_RESET_RANDOM_STATE = 1, /* uniform random cars/ball inside the field */
+    RSB_RESET_HIGH_CONTACT = 2  /* cars near the ball / each other, fast, half airborne */
+};
+
+typedef struct rsb_vec3 { float x, y, z; } rsb_vec3;
+
+/* Rows of RocketSim's RotMat: forward, right, up. */
+typedef struct rsb_rotmat { rsb_vec3 forward, right, up; } rsb_rotmat;
+
+/* RocketSim CarControls (Sim/CarControls.h). 24 bytes. */
+typedef struct rsb_controls {
+    float throttle, steer, pitch, yaw, roll;
+    uint8_t jump, boost, handbrake, pad_;
+} rsb_controls;
+
+/* RocketSim CarState (Sim/Car/Car.h:15-100) plus BallHitInfo. */
+typedef struct rsb_car_state {
+    rsb_vec3 pos;
+    rsb_rotmat rot;
+    rsb_vec3 vel;
+    rsb_vec3 ang_vel;          /* rad/s */
+    float boost;               /* 0..100 */
+    float time_spent_boosting;
+    float jump_time, flip_time, air_time, air_time_since_jump;
+    float supersonic_time, handbrake_val;
+    float auto_flip_timer, auto_flip_torque_scale;
+    float demo_respawn_timer;
+    float car_contact_cooldown;
+    rsb_vec3 flip_rel_torque;
+    rsb_vec3 world_contact_normal;
+    uint32_t car_contact_other_id;
+    uint8_t is_on_ground, has_jumped, has_double_jumped, has_flipped;
+    uint8_t is_flipping, is_jumping, is_supersonic, is_auto_flipping;
+    uint8_t is_demoed, world_contact, ball_hit_valid, team; /* team: 0 blue, 1 orange */
+    uint8_t wheels_with_contact[4];
+    uint64_t ball_hit_tick;          /* ~0 when never */
+    uint64_t ball_hit_extra_tick;    /* tick of the last extra car-ball impulse, ~0 when never */
+    rsb_vec3 ball_hit_rel_pos, ball_hit_ball_pos, ball_hit_extra_vel;
+    rsb_controls last_controls;
+    uint32_t id;
+    uint32_t pad_;
+} rsb_car_state;
+
+/* RocketSim BallState (Sim/Ball/Ball.h:15-45), soccar fields. */
+typedef struct rsb_ball_state {
+    rsb_vec3 pos;
+    rsb_rotmat rot;
+    rsb_vec3 vel;
+    rsb_vec3 ang_vel;
+} rsb_ball_state;
+
+/* RocketSim BoostPadState (Sim/BoostPad/BoostPad.h:21-30). */
+typedef struct rsb_pad_state {
+    uint8_t is_active;
+    uint8_t pad_[3];
+    float cooldown;
+    uint32_t prev_locked_car_id;  /* 0 = none */
+} rsb_pad_state;
+
+typedef struct rsb_arena_info {
+    uint64_t tick_count;
+    int32_t num_cars;
+    int32_t team_size;
+    int32_t goal_scored;   /* 1 while the ball is past a goal line (Arena::IsBallScored) */
+    int32_t goal_team;     /* team that scored: 0 blue, 1 orange, -1 none */
+    int32_t episode_ticks; /* ticks since the last reset, for the timeout terminal */
+    int32_t status;        /* per-arena status bits, RSB_ARENA_* */
+} rsb_arena_info;
+
+/* Per-arena status bits (rsb_arena_info.status). */
+enum {
+    RSB_ARENA_NONFINITE = 1,       /* NaN/Inf appeared in the state; arena should be reset */
+    RSB_ARENA_ROW_OVERFLOW = 2,    /* more solver rows than the fixed pool; extra contacts dropped */
+    RSB_ARENA_BVH_OVERFLOW = 4,    /* BVH traversal stack overflowed; query fell back to a linear scan */
+    RSB_ARENA_CULL_MISS = 8        /* the learned culler skipped a query that had a contact */
+};
+
+/* RocketSim MutatorConfig (Sim/MutatorConfig/MutatorConfig.h:16-70), soccar defaults when NULL. */
+typedef struct rsb_mutators {
+    rsb_vec3 gravity;
+    float car_mass, car_world_friction, car_world_restitution;
+    float ball_mass, ball_max_speed, ball_drag, ball_world_friction, ball_world_restitution;
+    float jump_accel, jump_immediate_force;
+    float boost_accel_ground, boost_accel_air, boost_used_per_second;
+    float respawn_delay, bump_cooldown_time;
+    float boost_pad_cooldown_big, boost_pad_cooldown_small, car_spawn_boost_amount;
+    float ball_hit_extra_force_scale, bump_force_scale, ball_radius;
+    uint8_t unlimited_flips, unlimited_double_jumps, demo_mode, enable_team_demos;
+    float goal_base_threshold_y;
+} rsb_mutators;
+
+/* The four stub rewards of the collector (CommonRewards.h) plus terminal settings. */
+typedef struct rsb_reward_config {
+    float w_goal;                 /* GoalReward */
+    float w_touch;                /* TouchBallReward */
+    float w_vel_ball_to_goal;     /* VelocityBallToGoalReward */
+    float w_vel_player_to_ball;   /* VelocityPlayerToBallReward */
+    float goal_concede_scale;     /* GoalReward's concedeScale (default -1) */
+    float team_spirit;            /* ZeroSumReward teamSpirit */
+    float opponent_scale;         /* ZeroSumReward opponentScale */
+    int32_t zero_sum;             /* 1: wrap rewards in ZeroSumReward */
+    int32_t episode_max_ticks;    /* timeout terminal (0 = off) */
+    float no_touch_timeout_s;     /* NoTouchCondition (0 = off) */
+} rsb_reward_config;
+
+typedef struct rsb_config {
+    int32_t num_arenas;
+    int32_t team_size;              /* used when team_sizes is NULL: 1, 2 or 3 */
+    const int32_t* team_sizes;      /* optional [num_arenas], each 1..3 (ragged batches) */
+    float tick_rate;                /* must be 120 */
+    int32_t tick_skip;              /* env step length in ticks (for rewards), e.g. 8 */
+    const char* meshes_path;        /* folder holding soccar/mesh_*.cmf (required) */
+    const rsb_mutators* mutators;   /* NULL = soccar defaults */
+    const rsb_reward_config* rewards; /* NULL = no rewards / terminals */
+    int32_t cull_mode;              /* RSB_CULL_* */
+    float cull_margin;              /* uu added to the learned bound before skipping */
+    uint64_t seed;
+    int32_t device;                 /* CUDA device ordinal */
+    int32_t threads;                /* host threads (CPU implementations only; 0 = all) */
+} rsb_config;
+
+typedef struct rsb_stats {
+    uint64_t ticks_simulated;       /* arena-ticks */
+    uint64_t narrowphase_queries;   /* ball/car vs arena-mesh queries */
+    uint64_t culled_queries;        /* queries skipped by the learned bound */
+    uint64_t missed_contacts;       /* culled queries that had a contact (audited) */
+    uint64_t solver_rows;           /* contact rows solved */
+    uint64_t arenas_reverted;       /* arenas switched back to the exact path */
+    uint64_t status_bits_seen;      /* OR of all rsb_arena_info.status bits */
+} rsb_stats;
+
+typedef struct rsb_handle rsb_handle;
+
+/* Fills *m with RocketSim's soccar MutatorConfig defaults. */
+rsb_status rsb_default_mutators(rsb_mutators* m);
+/* Fills *r with the collector's stub-reward defaults (all weights 1, zero-sum off). */
+rsb_status rsb_default_rewards(rsb_reward_config* r);
+
+rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out);
+rsb_status rsb_destroy(rsb_handle* h);
+
+/* Layout: car_offset has num_arenas+1 entries, team_size num_arenas. Either may be NULL. */
+rsb_status rsb_layout(const rsb_handle* h, int32_t* num_arenas, int32_t* num_cars,
+                      int32_t* car_offset, int32_t* team_size);
+/* AdvancedObs row stride (floats) of the obs buffer: 51 + 29 * max cars per arena. */
+rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride);
+
+rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode);
+rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* arena_idx, int32_t n,
+                            uint64_t seed, int32_t mode);
+
+rsb_status rsb_set_action_lut(rsb_handle* h, const rsb_controls* lut, int32_t count);
+/* Fills lut[90] with RLGymCPP's DefaultAction table. */
+rsb_status rsb_default_action_lut(rsb_controls* lut, int32_t count);
+rsb_status rsb_set_actions_host(rsb_handle* h, const int32_t* idx, int32_t n);
+rsb_status rsb_set_actions_device(rsb_handle* h, const int32_t* d_idx, int32_t n, void* stream);
+rsb_status rsb_set_controls(rsb_handle* h, const rsb_controls* controls, int32_t n);
+
+rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream);
+
+rsb_status rsb_snapshot(rsb_handle* h, void* stream);
+rsb_status rsb_build_obs(rsb_handle* h, void* stream);
+rsb_status rsb_build_rewards_terminals(rsb_handle* h, int32_t step_ticks, void* stream);
+
+rsb_status rsb_copy_obs(rsb_handle* h, float* out, size_t count);
+rsb_status rsb_copy_masks(rsb_handle* h, uint8_t* out, size_t count);
+rsb_status rsb_copy_rewards(rsb_handle* h, float* out, size_t count);
+rsb_status rsb_copy_terminals(rsb_handle* h, uint8_t* out, size_t count);
+rsb_status rsb_device_ptr(rsb_handle* h, int32_t which, void** out);
+
+rsb_status rsb_get_cars(rsb_handle* h, rsb_car_state* out, int32_t n);
+rsb_status rsb_set_cars(rsb_handle* h, const rsb_car_state* in, int32_t n);
+rsb_status rsb_get_balls(rsb_handle* h, rsb_ball_state* out, int32_t n);
+rsb_status rsb_set_balls(rsb_handle* h, const rsb_ball_state* in, int32_t n);
+rsb_status rsb_get_pads(rsb_handle* h, rsb_pad_state* out, int32_t n);   /* n = arenas * 34 */
+rsb_status rsb_set_pads(rsb_handle* h, const rsb_pad_state* in, int32_t n);
+rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n);
+
+rsb_status rsb_sync(rsb_handle* h);
+rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out);
+/* Copies the last error message (NUL-terminated, truncated to n). Safe with h == NULL
+   (returns the last rsb_create failure). */
+rsb_status rsb_last_error(const rsb_handle* h, char* buf, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSB_H */

@@ -1,0 +1,441 @@
+// ORACLE — test infrastructure only.  Puts the reference CPU RocketSim
+// (GigaLearnCPP/RLGymCPP/RocketSim, built from the reference's own sources by
+// oracle/Makefile) behind the engine's C ABI (include/rsb.h), so that every test
+// and the CPU-baseline leg of the benchmark can drive the reference and the CUDA
+// engine through identical calls.  Nothing in the product links this file.
+//
+// Reference behaviour followed:
+//   - RocketSim::InitFromMem            RocketSim.cpp:102-212 (meshes fed in mesh_0..mesh_15
+//                                       numeric order, so that the collision-object order,
+//                                       and hence Bullet's pair/manifold order, is fixed
+//                                       instead of following directory_iterator order)
+//   - Arena::Create / AddCar / Step     Arena.cpp:48-60, 716-812
+//   - Car::GetState / SetState          Car.cpp:9-35
+//   - Ball::GetState / SetState         Ball.cpp:27-49
+//   - BoostPad::GetState / SetState     BoostPad.h:45-46
+//   - Arena::IsBallScored               Arena.cpp:949-957
+#include "rsb.h"
+
+#include "RocketSim.h"
+
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace RocketSim;
+
+struct rsb_handle {
+    std::vector<Arena*> arenas;
+    std::vector<std::vector<Car*>> cars;  // per arena, blue first then orange
+    std::vector<int32_t> teamSize;
+    std::vector<int32_t> carOffset;
+    std::vector<rsb_controls> lut;
+    std::vector<rsb_controls> controls;
+    std::vector<int32_t> episodeTicks;
+    int32_t numCars = 0;
+    int32_t threads = 1;
+    std::string err;
+    rsb_stats stats{};
+};
+
+static std::string g_createError;
+static std::mutex g_initMutex;
+static bool g_inited = false;
+
+static rsb_status fail(rsb_handle* h, rsb_status code, const std::string& msg) {
+    if (h) h->err = msg; else g_createError = msg;
+    return code;
+}
+
+static bool initMeshes(const char* path, std::string& err) {
+    std::lock_guard<std::mutex> lock(g_initMutex);
+    if (g_inited) return true;
+    std::vector<FileData> files;
+    for (int i = 0; i < 64; i++) {
+        std::filesystem::path p = std::filesystem::path(path) / "soccar" / ("mesh_" + std::to_string(i) + ".cmf");
+        if (!std::filesystem::exists(p)) break;
+        std::ifstream f(p, std::ios::binary);
+        FileData d((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+        files.push_back(std::move(d));
+    }
+    if (files.empty()) {
+        err = std::string("no soccar/mesh_<i>.cmf under ") + path;
+        return false;
+    }
+    std::map<GameMode, std::vector<FileData>> m;
+    m[GameMode::SOCCAR] = files;
+    RocketSim::InitFromMem(m, true);
+    g_inited = true;
+    return true;
+}
+
+static Vec toVec(const rsb_vec3& v) { return Vec(v.x, v.y, v.z); }
+static rsb_vec3 fromVec(const Vec& v) { return rsb_vec3{v.x, v.y, v.z}; }
+
+static CarControls toControls(const rsb_controls& c) {
+    CarControls r;
+    r.throttle = c.throttle; r.steer = c.steer; r.pitch = c.pitch; r.yaw = c.yaw; r.roll = c.roll;
+    r.jump = c.jump != 0; r.boost = c.boost != 0; r.handbrake = c.handbrake != 0;
+    return r;
+}
+static rsb_controls fromControls(const CarControls& c) {
+    rsb_controls r{};
+    r.throttle = c.throttle; r.steer = c.steer; r.pitch = c.pitch; r.yaw = c.yaw; r.roll = c.roll;
+    r.jump = c.jump; r.boost = c.boost; r.handbrake = c.handbrake;
+    return r;
+}
+
+static rsb_car_state fromCarState(const CarState& s, Team team, uint32_t id) {
+    rsb_car_state o{};
+    o.pos = fromVec(s.pos);
+    o.rot.forward = fromVec(s.rotMat.forward);
+    o.rot.right = fromVec(s.rotMat.right);
+    o.rot.up = fromVec(s.rotMat.up);
+    o.vel = fromVec(s.vel);
+    o.ang_vel = fromVec(s.angVel);
+    o.boost = s.boost;
+    o.time_spent_boosting = s.timeSpentBoosting;
+    o.jump_time = s.jumpTime; o.flip_time = s.flipTime;
+    o.air_time = s.airTime; o.air_time_since_jump = s.airTimeSinceJump;
+    o.supersonic_time = s.supersonicTime; o.handbrake_val = s.handbrakeVal;
+    o.auto_flip_timer = s.autoFlipTimer; o.auto_flip_torque_scale = s.autoFlipTorqueScale;
+    o.demo_respawn_timer = s.demoRespawnTimer;
+    o.car_contact_cooldown = s.carContact.cooldownTimer;
+    o.flip_rel_torque = fromVec(s.flipRelTorque);
+    o.world_contact_normal = fromVec(s.worldContact.contactNormal);
+    o.car_contact_other_id = s.carContact.otherCarID;
+    o.is_on_ground = s.isOnGround; o.has_jumped = s.hasJumped;
+    o.has_double_jumped = s.hasDoubleJumped; o.has_flipped = s.hasFlipped;
+    o.is_flipping = s.isFlipping; o.is_jumping = s.isJumping;
+    o.is_supersonic = s.isSupersonic; o.is_auto_flipping = s.isAutoFlipping;
+    o.is_demoed = s.isDemoed; o.world_contact = s.worldContact.hasContact;
+    o.ball_hit_valid = s.ballHitInfo.isValid;
+    o.team = (team == Team::BLUE) ? 0 : 1;
+    for (int i = 0; i < 4; i++) o.wheels_with_contact[i] = s.wheelsWithContact[i];
+    o.ball_hit_tick = s.ballHitInfo.tickCountWhenHit;
+    o.ball_hit_extra_tick = s.ballHitInfo.tickCountWhenExtraImpulseApplied;
+    o.ball_hit_rel_pos = fromVec(s.ballHitInfo.relativePosOnBall);
+    o.ball_hit_ball_pos = fromVec(s.ballHitInfo.ballPos);
+    o.ball_hit_extra_vel = fromVec(s.ballHitInfo.extraHitVel);
+    o.last_controls = fromControls(s.lastControls);
+    o.id = id;
+    return o;
+}
+
+static CarState toCarState(const rsb_car_state& o) {
+    CarState s;
+    s.pos = toVec(o.pos);
+    s.rotMat = RotMat(toVec(o.rot.forward), toVec(o.rot.right), toVec(o.rot.up));
+    s.vel = toVec(o.vel);
+    s.angVel = toVec(o.ang_vel);
+    s.boost = o.boost;
+    s.timeSpentBoosting = o.time_spent_boosting;
+    s.jumpTime = o.jump_time; s.flipTime = o.flip_time;
+    s.airTime = o.air_time; s.airTimeSinceJump = o.air_time_since_jump;
+    s.supersonicTime = o.supersonic_time; s.handbrakeVal = o.handbrake_val;
+    s.autoFlipTimer = o.auto_flip_timer; s.autoFlipTorqueScale = o.auto_flip_torque_scale;
+    s.demoRespawnTimer = o.demo_respawn_timer;
+    s.carContact.cooldownTimer = o.car_contact_cooldown;
+    s.flipRelTorque = toVec(o.flip_rel_torque);
+    s.worldContact.contactNormal = toVec(o.world_contact_normal);
+    s.carContact.otherCarID = o.car_contact_other_id;
+    s.isOnGround = o.is_on_ground; s.hasJumped = o.has_jumped;
+    s.hasDoubleJumped = o.has_double_jumped; s.hasFlipped = o.has_flipped;
+    s.isFlipping = o.is_flipping; s.isJumping = o.is_jumping;
+    s.isSupersonic = o.is_supersonic; s.isAutoFlipping = o.is_auto_flipping;
+    s.isDemoed = o.is_demoed; s.worldContact.hasContact = o.world_contact;
+    s.ballHitInfo.isValid = o.ball_hit_valid;
+    for (int i = 0; i < 4; i++) s.wheelsWithContact[i] = o.wheels_with_contact[i];
+    s.ballHitInfo.tickCountWhenHit = o.ball_hit_tick;
+    s.ballHitInfo.tickCountWhenExtraImpulseApplied = o.ball_hit_extra_tick;
+    s.ballHitInfo.relativePosOnBall = toVec(o.ball_hit_rel_pos);
+    s.ballHitInfo.ballPos = toVec(o.ball_hit_ball_pos);
+    s.ballHitInfo.extraHitVel = toVec(o.ball_hit_extra_vel);
+    s.lastControls = toControls(o.last_controls);
+    return s;
+}
+
+extern "C" {
+
+rsb_status rsb_default_mutators(rsb_mutators* m) {
+    if (!m) return RSB_ERR_INVALID;
+    MutatorConfig d(GameMode::SOCCAR);
+    m->gravity = fromVec(d.gravity);
+    m->car_mass = d.carMass; m->car_world_friction = d.carWorldFriction;
+    m->car_world_restitution = d.carWorldRestitution;
+    m->ball_mass = d.ballMass; m->ball_max_speed = d.ballMaxSpeed; m->ball_drag = d.ballDrag;
+    m->ball_world_friction = d.ballWorldFriction; m->ball_world_restitution = d.ballWorldRestitution;
+    m->jump_accel = d.jumpAccel; m->jump_immediate_force = d.jumpImmediateForce;
+    m->boost_accel_ground = d.boostAccelGround; m->boost_accel_air = d.boostAccelAir;
+    m->boost_used_per_second = d.boostUsedPerSecond;
+    m->respawn_delay = d.respawnDelay; m->bump_cooldown_time = d.bumpCooldownTime;
+    m->boost_pad_cooldown_big = d.boostPadCooldown_Big;
+    m->boost_pad_cooldown_small = d.boostPadCooldown_Small;
+    m->car_spawn_boost_amount = d.carSpawnBoostAmount;
+    m->ball_hit_extra_force_scale = d.ballHitExtraForceScale;
+    m->bump_force_scale = d.bumpForceScale; m->ball_radius = d.ballRadius;
+    m->unlimited_flips = d.unlimitedFlips; m->unlimited_double_jumps = d.unlimitedDoubleJumps;
+    m->demo_mode = (uint8_t)d.demoMode; m->enable_team_demos = d.enableTeamDemos;
+    m->goal_base_threshold_y = d.goalBaseThresholdY;
+    return RSB_OK;
+}
+
+static MutatorConfig toMutators(const rsb_mutators& m) {
+    MutatorConfig d(GameMode::SOCCAR);
+    d.gravity = toVec(m.gravity);
+    d.carMass = m.car_mass; d.carWorldFriction = m.car_world_friction;
+    d.carWorldRestitution = m.car_world_restitution;
+    d.ballMass = m.ball_mass; d.ballMaxSpeed = m.ball_max_speed; d.ballDrag = m.ball_drag;
+    d.ballWorldFriction = m.ball_world_friction; d.ballWorldRestitution = m.ball_world_restitution;
+    d.jumpAccel = m.jump_accel; d.jumpImmediateForce = m.jump_immediate_force;
+    d.boostAccelGround = m.boost_accel_ground; d.boostAccelAir = m.boost_accel_air;
+    d.boostUsedPerSecond = m.boost_used_per_second;
+    d.respawnDelay = m.respawn_delay; d.bumpCooldownTime = m.bump_cooldown_time;
+    d.boostPadCooldown_Big = m.boost_pad_cooldown_big;
+    d.boostPadCooldown_Small = m.boost_pad_cooldown_small;
+    d.carSpawnBoostAmount = m.car_spawn_boost_amount;
+    d.ballHitExtraForceScale = m.ball_hit_extra_force_scale;
+    d.bumpForceScale = m.bump_force_scale; d.ballRadius = m.ball_radius;
+    d.unlimitedFlips = m.unlimited_flips; d.unlimitedDoubleJumps = m.unlimited_double_jumps;
+    d.demoMode = (DemoMode)m.demo_mode; d.enableTeamDemos = m.enable_team_demos;
+    d.goalBaseThresholdY = m.goal_base_threshold_y;
+    return d;
+}
+
+rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
+    if (!cfg || !out) return fail(nullptr, RSB_ERR_INVALID, "null config or output");
+    *out = nullptr;
+    if (cfg->num_arenas <= 0) return fail(nullptr, RSB_ERR_INVALID, "num_arenas must be > 0");
+    if (!cfg->meshes_path) return fail(nullptr, RSB_ERR_MESH, "meshes_path is required");
+    if (cfg->tick_rate != 120.f) return fail(nullptr, RSB_ERR_UNSUPPORTED, "tick_rate must be 120");
+    std::string err;
+    if (!initMeshes(cfg->meshes_path, err)) return fail(nullptr, RSB_ERR_MESH, err);
+
+    rsb_handle* h = new rsb_handle();
+    h->threads = cfg->threads > 0 ? cfg->threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    h->carOffset.push_back(0);
+    for (int a = 0; a < cfg->num_arenas; a++) {
+        int ts = cfg->team_sizes ? cfg->team_sizes[a] : cfg->team_size;
+        if (ts < 1 || ts > RSB_MAX_TEAM_SIZE) {
+            delete h;
+            return fail(nullptr, RSB_ERR_INVALID, "team size must be 1..3");
+        }
+        h->teamSize.push_back(ts);
+        h->carOffset.push_back(h->carOffset.back() + 2 * ts);
+    }
+    h->numCars = h->carOffset.back();
+    MutatorConfig mut(GameMode::SOCCAR);
+    if (cfg->mutators) mut = toMutators(*cfg->mutators);
+    h->arenas.resize(cfg->num_arenas);
+    h->cars.resize(cfg->num_arenas);
+    for (int a = 0; a < cfg->num_arenas; a++) {
+        Arena* arena = Arena::Create(GameMode::SOCCAR);
+        arena->SetMutatorConfig(mut);
+        for (int t = 0; t < 2; t++)
+            for (int i = 0; i < h->teamSize[a]; i++)
+                h->cars[a].push_back(arena->AddCar(t == 0 ? Team::BLUE : Team::ORANGE));
+        h->arenas[a] = arena;
+    }
+    h->controls.assign(h->numCars, rsb_controls{});
+    h->episodeTicks.assign(cfg->num_arenas, 0);
+    *out = h;
+    return RSB_OK;
+}
+
+rsb_status rsb_destroy(rsb_handle* h) {
+    if (!h) return RSB_ERR_INVALID;
+    for (Arena* a : h->arenas) delete a;
+    delete h;
+    return RSB_OK;
+}
+
+rsb_status rsb_layout(const rsb_handle* h, int32_t* num_arenas, int32_t* num_cars,
+                      int32_t* car_offset, int32_t* team_size) {
+    if (!h) return RSB_ERR_INVALID;
+    if (num_arenas) *num_arenas = (int32_t)h->arenas.size();
+    if (num_cars) *num_cars = h->numCars;
+    if (car_offset) std::memcpy(car_offset, h->carOffset.data(), h->carOffset.size() * sizeof(int32_t));
+    if (team_size) std::memcpy(team_size, h->teamSize.data(), h->teamSize.size() * sizeof(int32_t));
+    return RSB_OK;
+}
+
+rsb_status rsb_set_controls(rsb_handle* h, const rsb_controls* c, int32_t n) {
+    if (!h || !c || n != h->numCars) return fail(h, RSB_ERR_INVALID, "controls count must equal num_cars");
+    std::memcpy(h->controls.data(), c, sizeof(rsb_controls) * n);
+    return RSB_OK;
+}
+
+rsb_status rsb_set_action_lut(rsb_handle* h, const rsb_controls* lut, int32_t count) {
+    if (!h || !lut || count <= 0) return fail(h, RSB_ERR_INVALID, "bad action table");
+    h->lut.assign(lut, lut + count);
+    return RSB_OK;
+}
+
+rsb_status rsb_set_actions_host(rsb_handle* h, const int32_t* idx, int32_t n) {
+    if (!h || !idx || n != h->numCars) return fail(h, RSB_ERR_INVALID, "action count must equal num_cars");
+    if (h->lut.empty()) return fail(h, RSB_ERR_STATE, "no action table");
+    int last = (int)h->lut.size() - 1;
+    for (int i = 0; i < n; i++) {
+        int k = idx[i] < 0 ? 0 : (idx[i] > last ? last : idx[i]);
+        h->controls[i] = h->lut[k];
+    }
+    return RSB_OK;
+}
+
+static void stepRange(rsb_handle* h, int a0, int a1, int ticks) {
+    for (int a = a0; a < a1; a++) {
+        auto& cars = h->cars[a];
+        for (size_t c = 0; c < cars.size(); c++)
+            cars[c]->controls = toControls(h->controls[h->carOffset[a] + c]);
+        h->arenas[a]->Step(ticks);
+        h->episodeTicks[a] += ticks;
+    }
+}
+
+rsb_status rsb_step(rsb_handle* h, int32_t ticks, void*) {
+    if (!h || ticks < 0) return fail(h, RSB_ERR_INVALID, "bad tick count");
+    int n = (int)h->arenas.size();
+    int t = std::min(h->threads, n);
+    if (t <= 1) {
+        stepRange(h, 0, n, ticks);
+    } else {
+        std::vector<std::thread> pool;
+        std::atomic<int> next{0};
+        const int chunk = 4;
+        for (int i = 0; i < t; i++)
+            pool.emplace_back([&] {
+                for (;;) {
+                    int a0 = next.fetch_add(chunk);
+                    if (a0 >= n) break;
+                    stepRange(h, a0, std::min(n, a0 + chunk), ticks);
+                }
+            });
+        for (auto& th : pool) th.join();
+    }
+    h->stats.ticks_simulated += (uint64_t)n * ticks;
+    return RSB_OK;
+}
+
+rsb_status rsb_get_cars(rsb_handle* h, rsb_car_state* out, int32_t n) {
+    if (!h || !out || n != h->numCars) return fail(h, RSB_ERR_INVALID, "car count must equal num_cars");
+    for (size_t a = 0; a < h->arenas.size(); a++)
+        for (size_t c = 0; c < h->cars[a].size(); c++) {
+            Car* car = h->cars[a][c];
+            out[h->carOffset[a] + c] = fromCarState(car->GetState(), car->team, car->id);
+        }
+    return RSB_OK;
+}
+
+rsb_status rsb_set_cars(rsb_handle* h, const rsb_car_state* in, int32_t n) {
+    if (!h || !in || n != h->numCars) return fail(h, RSB_ERR_INVALID, "car count must equal num_cars");
+    for (size_t a = 0; a < h->arenas.size(); a++)
+        for (size_t c = 0; c < h->cars[a].size(); c++)
+            h->cars[a][c]->SetState(toCarState(in[h->carOffset[a] + c]));
+    return RSB_OK;
+}
+
+rsb_status rsb_get_balls(rsb_handle* h, rsb_ball_state* out, int32_t n) {
+    if (!h || !out || n != (int32_t)h->arenas.size()) return fail(h, RSB_ERR_INVALID, "ball count must equal num_arenas");
+    for (int a = 0; a < n; a++) {
+        BallState s = h->arenas[a]->ball->GetState();
+        out[a].pos = fromVec(s.pos);
+        out[a].rot.forward = fromVec(s.rotMat.forward);
+        out[a].rot.right = fromVec(s.rotMat.right);
+        out[a].rot.up = fromVec(s.rotMat.up);
+        out[a].vel = fromVec(s.vel);
+        out[a].ang_vel = fromVec(s.angVel);
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_set_balls(rsb_handle* h, const rsb_ball_state* in, int32_t n) {
+    if (!h || !in || n != (int32_t)h->arenas.size()) return fail(h, RSB_ERR_INVALID, "ball count must equal num_arenas");
+    for (int a = 0; a < n; a++) {
+        BallState s;
+        s.pos = toVec(in[a].pos);
+        s.rotMat = RotMat(toVec(in[a].rot.forward), toVec(in[a].rot.right), toVec(in[a].rot.up));
+        s.vel = toVec(in[a].vel);
+        s.angVel = toVec(in[a].ang_vel);
+        h->arenas[a]->ball->SetState(s);
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_get_pads(rsb_handle* h, rsb_pad_state* out, int32_t n) {
+    if (!h || !out || n != (int32_t)h->arenas.size() * RSB_NUM_PADS) return fail(h, RSB_ERR_INVALID, "pad count must equal num_arenas*34");
+    for (size_t a = 0; a < h->arenas.size(); a++) {
+        auto& pads = h->arenas[a]->GetBoostPads();
+        for (int p = 0; p < RSB_NUM_PADS; p++) {
+            BoostPadState s = pads[p]->GetState();
+            rsb_pad_state& o = out[a * RSB_NUM_PADS + p];
+            o = rsb_pad_state{};
+            o.is_active = s.isActive;
+            o.cooldown = s.cooldown;
+            o.prev_locked_car_id = s.prevLockedCarID;
+        }
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_set_pads(rsb_handle* h, const rsb_pad_state* in, int32_t n) {
+    if (!h || !in || n != (int32_t)h->arenas.size() * RSB_NUM_PADS) return fail(h, RSB_ERR_INVALID, "pad count must equal num_arenas*34");
+    for (size_t a = 0; a < h->arenas.size(); a++) {
+        auto& pads = h->arenas[a]->GetBoostPads();
+        for (int p = 0; p < RSB_NUM_PADS; p++) {
+            const rsb_pad_state& o = in[a * RSB_NUM_PADS + p];
+            BoostPadState s;
+            s.isActive = o.is_active;
+            s.cooldown = o.cooldown;
+            s.prevLockedCarID = o.prev_locked_car_id;
+            pads[p]->SetState(s);
+        }
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
+    if (!h || !out || n != (int32_t)h->arenas.size()) return fail(h, RSB_ERR_INVALID, "info count must equal num_arenas");
+    for (int a = 0; a < n; a++) {
+        Arena* ar = h->arenas[a];
+        rsb_arena_info& o = out[a];
+        o = rsb_arena_info{};
+        o.tick_count = ar->tickCount;
+        o.num_cars = 2 * h->teamSize[a];
+        o.team_size = h->teamSize[a];
+        bool scored = ar->IsBallScored();
+        o.goal_scored = scored;
+        float y = ar->ball->GetState().pos.y;
+        // RS_TEAM_FROM_Y(-y): the ball past +y scores for blue (orange's net is at +y)
+        o.goal_team = scored ? (y > 0 ? 0 : 1) : -1;
+        o.episode_ticks = h->episodeTicks[a];
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_sync(rsb_handle* h) { return h ? RSB_OK : RSB_ERR_INVALID; }
+
+rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out) {
+    if (!h || !out) return RSB_ERR_INVALID;
+    *out = h->stats;
+    return RSB_OK;
+}
+
+rsb_status rsb_last_error(const rsb_handle* h, char* buf, size_t n) {
+    if (!buf || n == 0) return RSB_ERR_INVALID;
+    const std::string& s = h ? h->err : g_createError;
+    std::snprintf(buf, n, "%s", s.c_str());
+    return RSB_OK;
+}
+
+rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride) {
+    if (!h || !stride) return RSB_ERR_INVALID;
+    int m = 0;
+    for (int t : h->teamSize) m = std::max(m, 2 * t);
+    *stride = RSB_OBS_BASE + RSB_OBS_PER_CAR * m;
+    return RSB_OK;
+}
+
+}  // extern "C"

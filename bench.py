@@ -1,0 +1,284 @@
+"""Throughput benchmark: arena-ticks/s of the batched soccar simulator on B200.
+
+One step = one env step of every arena: actions in, `tick_skip` physics ticks, state
+out.  Timing follows the measurement contract: W untimed warm-up steps, then K steps,
+each bracketed by CUDA events on the stream the kernels run on, the L2 flushed
+(256 MB write) between timed steps, max over ranks.  `--impl reference` times the
+reference's own CPU RocketSim (oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "emy-s-framework_b200")
+ORACLE_LIB = os.path.join(ROOT, "oracle", "_ref", "librsref.so")
+METRIC = "arena-ticks/s on 1 B200, learned-cull vs exact-BVH path; % of HBM roofline"
+
+
+def load_pkg():
+    name = "emy_s_framework_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.stop_ev = threading.Event()
+        self.thread = None
+
+    def _run(self):
+        while not self.stop_ev.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([s.strip() for s in out.split(",")])
+            except Exception:
+                pass
+            self.stop_ev.wait(0.2)
+
+    def __enter__(self):
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop_ev.set()
+        if self.thread:
+            self.thread.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, name in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------ workload
+
+class Workload:
+    """The timed configuration.  Arenas without cars until the vehicle is built in."""
+
+    def __init__(self, args):
+        self.num_arenas = args.arenas
+        self.team_size = args.team_size
+        self.tick_skip = args.tick_skip
+        self.name = args.workload_name
+
+    def config(self):
+        return {"workload": self.name, "arenas": self.num_arenas, "team_size": self.team_size,
+                "tick_skip": self.tick_skip, "narrowphase": "exact-bvh", "state": "fp32",
+                "l2": "flushed between timed steps (256 MB write)"}
+
+
+def initial_balls(rsb, n, seed):
+    rng = np.random.default_rng(seed)
+    b = np.zeros(n, rsb.BALL_DTYPE)
+    for k, f in enumerate(("forward", "right", "up")):
+        for c in "xyz":
+            b["rot"][f][c] = 1.0 if "xyz"[k] == c else 0.0
+    b["pos"]["x"] = rng.uniform(-3500, 3500, n)
+    b["pos"]["y"] = rng.uniform(-4000, 4000, n)
+    b["pos"]["z"] = rng.uniform(100, 1820, n)
+    sp = rng.uniform(0, 3000, n)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    for k, c in enumerate("xyz"):
+        b["vel"][c] = d[:, k] * sp
+    return b
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    pkg = load_pkg()
+    rsb = pkg.rsb
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    wl = Workload(args)
+    batch = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size,
+                      meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank)
+    batch.set_balls(initial_balls(rsb, wl.num_arenas, 0x5EED0001 + rank))
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def one_step():
+        batch.step(wl.tick_skip, stream=sp)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            one_step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    times = []
+    with ClockSampler(dev) as clocks, torch.cuda.stream(stream):
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # evict the L2 between timed steps
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            one_step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+    total_ms = float(sum(times))
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    arena_ticks = wl.num_arenas * wl.tick_skip * args.steps * world
+    value = arena_ticks / (total_ms / 1e3)
+
+    # e2e through the public API with host buffers: step + host read of the arena infos
+    e2e_times = []
+    infos_bytes = wl.num_arenas * rsb.INFO_DTYPE.itemsize
+    for _ in range(max(3, min(args.steps, 10))):
+        t0 = time.perf_counter()
+        batch.step(wl.tick_skip)
+        batch.get_arena_info()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_value = wl.num_arenas * wl.tick_skip * world / statistics.median(e2e_times)
+
+    # roofline of the step kernel: algorithmic bytes = state read + written per launch
+    from ctypes import sizeof
+    state_bytes = wl.num_arenas * (sizeof(rsb.BallState) * 0 + 4 * (23 + 8))  # ball + arena words
+    alg_bytes = 2 * state_bytes
+    kernel_s = (total_ms / args.steps) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / kernel_s / 1e9
+    res = {
+        "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random states)",
+        "config": wl.config() | {"parallelism": f"arena-shards x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "bytes_per_launch": alg_bytes},
+        "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": infos_bytes},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+    }
+    return res
+
+
+# ------------------------------------------------------------------ CPU reference
+
+def cpu_reference(args, sample_s=10.0, threads=None):
+    pkg = load_pkg()
+    rsb = pkg.rsb
+    lib = rsb.load_library(ORACLE_LIB)
+    threads = threads or os.cpu_count() or 1
+    n = min(args.arenas, 64 * threads)
+    wl = Workload(args)
+    b = rsb.Batch(lib, n, team_size=wl.team_size, meshes_path=pkg.MESHES_DIR, threads=threads)
+    b.set_balls(initial_balls(rsb, n, 0x5EED0001))
+    b.step(wl.tick_skip)
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < sample_s:
+        b.step(wl.tick_skip)
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": n * wl.tick_skip * steps / dt, "unit": "arena-ticks/s", "cores": threads,
+            "kind": "reference", "sample": f"{n} arenas x {steps} env steps of {wl.tick_skip} ticks ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    cb = cpu_reference(args, sample_s=args.ref_seconds)
+    wl = Workload(args)
+    return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "arena-ticks/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random states)",
+            "config": wl.config(), "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "arena-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--arenas", type=int, default=8192)
+    ap.add_argument("--team-size", type=int, default=0)
+    ap.add_argument("--tick-skip", type=int, default=8)
+    ap.add_argument("--workload-name", default="soccar ball-only x 8192 arenas, tickSkip 8 (cars not built yet)")
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    res = run_ours(args, rank, world, dist)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            res["cpu_baseline"] = cpu_reference(args, sample_s=args.ref_seconds)
+        print(json.dumps(res), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -54,9 +54,16 @@ RSB_HD int sortCachedPoints(const Manifold& m, const MPoint& pt) {
 // Inserts a contact into manifold m.  res0/res1 are the btManifoldResult's bodies (the
 // pair order); the manifold's own body order decides the swap, as in the reference.
 // Returns the point slot, or -1 when the point is beyond the breaking threshold.
-RSB_HD int addContact(Manifold& m, int res0, const ObjRef& r0, int res1, const ObjRef& r1,
+RSB_HD int addContact(Manifold& m, BlockPool& pool, int res0, const ObjRef& r0, int res1, const ObjRef& r1,
                       V3 normalOnB, V3 pointInWorld, float depth) {
     if (depth > m.cbt) return -1;
+    if (!m.pt) {
+        if (pool.n >= MAX_BLOCKS) {
+            *pool.status |= 2u;  // row/contact pool overflow: contact dropped
+            return -1;
+        }
+        m.pt = pool.pts + MAX_POINTS * pool.n++;
+    }
     bool swapped = m.o0 != res0;
     V3 pointA = pointInWorld + normalOnB * depth;
     MPoint np;

@@ -20,6 +20,7 @@
 #endif
 
 #include <math.h>
+#include <string.h>
 
 namespace rsb {
 

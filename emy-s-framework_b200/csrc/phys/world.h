@@ -27,6 +27,7 @@ struct World {
     int16_t po0[MAX_PAIRS], po1[MAX_PAIRS];
     int nm;
     Manifold m[MAX_MANIFOLDS];
+    BlockPool pool;
     uint32_t status;
 };
 
@@ -314,7 +315,7 @@ RSB_HD void collideBallMesh(World& W, int mesh, Manifold& man) {
         V3 point, normal;
         float depth;
         if (sphereTriCollide(v, ball.xf.o, P.ballRadius, man.cbt, point, normal, depth)) {
-            int idx = addContact(man, mesh, rMesh, OBJ_BALL, rBall, normal, point, depth);
+            int idx = addContact(man, W.pool, mesh, rMesh, OBJ_BALL, rBall, normal, point, depth);
             if (idx >= 0) {
                 MPoint& cp = man.pt[idx];
                 cp.index1 = tri;
@@ -342,7 +343,7 @@ RSB_HD void collideBallPlane(World& W, int plane, Manifold& man) {
         V3 proj = vip - pn * distance;
         V3 world = xfPoint(rPlane.xf, proj);
         V3 nb = rPlane.xf.b * pn;
-        int idx = addContact(man, plane, rPlane, OBJ_BALL, rBall, nb, world, distance);
+        int idx = addContact(man, W.pool, plane, rPlane, OBJ_BALL, rBall, nb, world, distance);
         if (idx >= 0) man.pt[idx].special = 1;
     }
     if (man.n) refreshContactPoints(man, rBall.xf, rPlane.xf);
@@ -352,6 +353,8 @@ RSB_HD void collideBallPlane(World& W, int plane, Manifold& man) {
 
 RSB_HD void dispatchPairs(World& W) {
     W.nm = 0;
+    W.pool.n = 0;
+    W.pool.status = &W.status;
     for (int p = 0; p < W.np; p++) {
         int o0 = W.po0[p], o1 = W.po1[p];
         if (!objActive(W, o0) && !objActive(W, o1)) continue;  // needsCollision
@@ -362,6 +365,7 @@ RSB_HD void dispatchPairs(World& W) {
             man.o1 = o0;
             man.cbt = W.P->ballCbt;
             man.n = 0;
+            man.pt = nullptr;
             if (o0 < MAX_MESHES) collideBallMesh(W, o0, man);
             else collideBallPlane(W, o0, man);
         }

@@ -57,14 +57,21 @@ struct MPoint {
     int32_t special;
 };
 
-constexpr int MAX_MANIFOLDS = 48;
-constexpr int MAX_POINTS = 4;
+constexpr int MAX_MANIFOLDS = 64;   // headers, one per processed pair, in creation order
+constexpr int MAX_POINTS = 4;       // btPersistentManifold MANIFOLD_CACHE_SIZE
+constexpr int MAX_BLOCKS = 16;      // manifolds that hold contacts in one tick
 
 struct Manifold {
     int32_t o0, o1;   // object ids (body0 / body1)
     float cbt;        // contact breaking threshold
+    int32_t n;        // number of points
+    MPoint* pt;       // point block (4 slots), null until the first contact
+};
+
+struct BlockPool {
     int32_t n;
-    MPoint pt[MAX_POINTS];
+    uint32_t* status;
+    MPoint pts[MAX_BLOCKS * MAX_POINTS];
 };
 
 // btSolverConstraint fields used by contact and friction rows
@@ -105,7 +112,8 @@ struct WorldParams {
     V3 ballInvInertia;
     float ballFriction, ballRestitution;
     float ballMaxSpeedBt;
-    int32_t numDynProxiesExtra; // unused, keeps layout stable
+    float goalBaseY;          // mutator goalBaseThresholdY (uu)
+    float ballRadiusUu;
 };
 
 }  // namespace rsb

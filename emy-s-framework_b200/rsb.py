@@ -179,7 +179,7 @@ def load_library(path: str) -> C.CDLL:
     path = os.path.abspath(path)
     if path in _LIBS:
         return _LIBS[path]
-    lib = C.CDLL(path, mode=C.RTLD_GLOBAL)
+    lib = C.CDLL(path, mode=C.RTLD_LOCAL)
     for name, args in _SIGS.items():
         fn = getattr(lib, name, None)
         if fn is None:

@@ -219,9 +219,9 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     h->carOffset.push_back(0);
     for (int a = 0; a < cfg->num_arenas; a++) {
         int ts = cfg->team_sizes ? cfg->team_sizes[a] : cfg->team_size;
-        if (ts < 1 || ts > RSB_MAX_TEAM_SIZE) {
+        if (ts < 0 || ts > RSB_MAX_TEAM_SIZE) {
             delete h;
-            return fail(nullptr, RSB_ERR_INVALID, "team size must be 1..3");
+            return fail(nullptr, RSB_ERR_INVALID, "team size must be 0..3");
         }
         h->teamSize.push_back(ts);
         h->carOffset.push_back(h->carOffset.back() + 2 * ts);
@@ -437,5 +437,20 @@ rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride) {
     *stride = RSB_OBS_BASE + RSB_OBS_PER_CAR * m;
     return RSB_OK;
 }
+
+// Env-layer entry points (resets, observations, rewards) are added with the env layer.
+rsb_status rsb_default_rewards(rsb_reward_config*) { return RSB_ERR_UNSUPPORTED; }
+rsb_status rsb_reset_all(rsb_handle* h, uint64_t, int32_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t*, int32_t, uint64_t, int32_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_default_action_lut(rsb_controls*, int32_t) { return RSB_ERR_UNSUPPORTED; }
+rsb_status rsb_set_actions_device(rsb_handle* h, const int32_t*, int32_t, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "no device on the CPU oracle"); }
+rsb_status rsb_snapshot(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_build_obs(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_build_rewards_terminals(rsb_handle* h, int32_t, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_copy_obs(rsb_handle* h, float*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_copy_masks(rsb_handle* h, uint8_t*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_copy_rewards(rsb_handle* h, float*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_copy_terminals(rsb_handle* h, uint8_t*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
+rsb_status rsb_device_ptr(rsb_handle* h, int32_t, void**) { return fail(h, RSB_ERR_UNSUPPORTED, "no device on the CPU oracle"); }
 
 }  // extern "C"

@@ -1,0 +1,43 @@
+"""C ABI checks that need no GPU: both libraries load and export every symbol that
+include/rsb.h declares; the engine refuses to run without a CUDA device."""
+from __future__ import annotations
+
+import os
+import re
+
+import pytest
+
+from conftest import ORACLE_LIB, ROOT
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "rsb.h")).read()
+    return sorted(set(re.findall(r"^rsb_status\s+(rsb_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_header_matches_binding(pkg):
+    assert header_symbols() == sorted(pkg.rsb.ABI_SYMBOLS)
+
+
+@pytest.mark.parametrize("which", ["engine", "oracle"])
+def test_library_exports_every_symbol(pkg, which):
+    lib = pkg.engine_library() if which == "engine" else pkg.rsb.load_library(ORACLE_LIB)
+    missing = [s for s in header_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_engine_without_gpu_fails_loudly(pkg, meshes_dir):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pkg.rsb.RsbError) as e:
+        pkg.rsb.Batch(pkg.engine_library(), 2, team_size=0, meshes_path=meshes_dir)
+    assert e.value.code == -2  # RSB_ERR_CUDA: no CPU fallback exists
+
+
+def test_oracle_rejects_bad_config(pkg, oracle_lib, meshes_dir):
+    with pytest.raises(pkg.rsb.RsbError):
+        pkg.rsb.Batch(oracle_lib, 0, team_size=1, meshes_path=meshes_dir)
+    with pytest.raises(pkg.rsb.RsbError):
+        pkg.rsb.Batch(oracle_lib, 1, team_size=4, meshes_path=meshes_dir)

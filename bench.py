@@ -99,7 +99,9 @@ class ClockSampler:
 # ------------------------------------------------------------------ workload
 
 class Workload:
-    """The timed configuration.  Arenas without cars until the vehicle is built in."""
+    """The timed configuration: soccar arenas at seeded random states (cars on the ground,
+    random headings / speeds / boost, ball anywhere), a fresh discrete action per car from
+    the 90-entry table every env step."""
 
     def __init__(self, args):
         self.num_arenas = args.arenas
@@ -110,7 +112,27 @@ class Workload:
     def config(self):
         return {"workload": self.name, "arenas": self.num_arenas, "team_size": self.team_size,
                 "tick_skip": self.tick_skip, "narrowphase": "exact-bvh", "state": "fp32",
+                "actions": "uniform over the 90-action table, new each env step",
                 "l2": "flushed between timed steps (256 MB write)"}
+
+
+def initial_cars(cars, seed):
+    rng = np.random.default_rng(seed)
+    c = cars.copy()
+    n = len(c)
+    yaw = rng.uniform(-np.pi, np.pi, n)
+    cy, sy = np.cos(yaw), np.sin(yaw)
+    c["pos"]["x"] = rng.uniform(-3500, 3500, n)
+    c["pos"]["y"] = rng.uniform(-4500, 4500, n)
+    c["pos"]["z"] = 17.0
+    c["rot"]["forward"]["x"], c["rot"]["forward"]["y"], c["rot"]["forward"]["z"] = cy, sy, 0
+    c["rot"]["right"]["x"], c["rot"]["right"]["y"], c["rot"]["right"]["z"] = -sy, cy, 0
+    c["rot"]["up"]["x"], c["rot"]["up"]["y"], c["rot"]["up"]["z"] = 0, 0, 1
+    sp = rng.uniform(0, 2300, n)
+    c["vel"]["x"], c["vel"]["y"], c["vel"]["z"] = cy * sp, sy * sp, 0
+    c["boost"] = rng.uniform(0, 100, n)
+    c["is_on_ground"] = 1
+    return c
 
 
 def initial_balls(rsb, n, seed):
@@ -143,11 +165,22 @@ def run_ours(args, rank, world, dist):
     batch = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size,
                       meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank)
     batch.set_balls(initial_balls(rsb, wl.num_arenas, 0x5EED0001 + rank))
+    if batch.num_cars:
+        batch.set_cars(initial_cars(batch.get_cars(), 0x5EED0002 + rank))
+    batch.set_action_lut(rsb.default_action_lut(batch.lib))
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    gen = torch.Generator(device=f"cuda:{dev}")
+    gen.manual_seed(0x5EED0003 + rank)
+    n_cars = max(1, batch.num_cars)
+    actions = torch.empty(n_cars, dtype=torch.int32, device=dev)
 
     def one_step():
+        # the policy's actions arrive on the device; expand them and run tick_skip ticks
+        if batch.num_cars:
+            actions.random_(0, rsb.RSB_NUM_ACTIONS, generator=gen)
+            batch.set_actions_device(actions.data_ptr(), batch.num_cars, stream=sp)
         batch.step(wl.tick_skip, stream=sp)
 
     with torch.cuda.stream(stream):
@@ -178,20 +211,25 @@ def run_ours(args, rank, world, dist):
     arena_ticks = wl.num_arenas * wl.tick_skip * args.steps * world
     value = arena_ticks / (total_ms / 1e3)
 
-    # e2e through the public API with host buffers: step + host read of the arena infos
+    # e2e through the public API with host buffers: host actions in (H2D), step, host read
+    # of the arena infos (D2H)
     e2e_times = []
-    infos_bytes = wl.num_arenas * rsb.INFO_DTYPE.itemsize
-    for _ in range(max(3, min(args.steps, 10))):
+    infos_bytes = wl.num_arenas * 32  # rsb_get_arena_info copies the 8-word arena record per arena
+    rng = np.random.default_rng(0x5EED0004 + rank)
+    host_actions = rng.integers(0, rsb.RSB_NUM_ACTIONS, (16, n_cars)).astype(np.int32)
+    for k in range(max(3, min(args.steps, 10))):
         t0 = time.perf_counter()
+        if batch.num_cars:
+            batch.set_actions(host_actions[k % 16, :batch.num_cars])
         batch.step(wl.tick_skip)
         batch.get_arena_info()
         e2e_times.append(time.perf_counter() - t0)
     e2e_value = wl.num_arenas * wl.tick_skip * world / statistics.median(e2e_times)
+    h2d_bytes = 4 * batch.num_cars
 
-    # roofline of the step kernel: algorithmic bytes = state read + written per launch
-    from ctypes import sizeof
-    state_bytes = wl.num_arenas * (sizeof(rsb.BallState) * 0 + 4 * (23 + 8))  # ball + arena words
-    alg_bytes = 2 * state_bytes
+    # roofline of the step kernel: algorithmic bytes = persistent state read + written
+    # per launch (the library reports it)
+    alg_bytes = batch.stats()["state_bytes_per_step"]
     kernel_s = (total_ms / args.steps) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / kernel_s / 1e9
@@ -203,9 +241,9 @@ def run_ours(args, rank, world, dist):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                      "bytes_per_launch": alg_bytes},
-        "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d_bytes,
                 "d2h_bytes_per_step": infos_bytes},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (2 if batch.num_cars else 1),
         "clocks": clocks.summary(),
     }
     return res
@@ -222,10 +260,21 @@ def cpu_reference(args, sample_s=10.0, threads=None):
     wl = Workload(args)
     b = rsb.Batch(lib, n, team_size=wl.team_size, meshes_path=pkg.MESHES_DIR, threads=threads)
     b.set_balls(initial_balls(rsb, n, 0x5EED0001))
-    b.step(wl.tick_skip)
+    if b.num_cars:
+        b.set_cars(initial_cars(b.get_cars(), 0x5EED0002))
+    lut = rsb.default_action_table()
+    rng = np.random.default_rng(0x5EED0003)
+    pool = [lut[rng.integers(0, len(lut), max(1, b.num_cars))] for _ in range(16)]
+
+    def env_step(k):
+        if b.num_cars:
+            b.set_controls(pool[k % 16])
+        b.step(wl.tick_skip)
+
+    env_step(0)
     steps, t0 = 0, time.perf_counter()
     while time.perf_counter() - t0 < sample_s:
-        b.step(wl.tick_skip)
+        env_step(steps)
         steps += 1
     dt = time.perf_counter() - t0
     return {"value": n * wl.tick_skip * steps / dt, "unit": "arena-ticks/s", "cores": threads,
@@ -249,9 +298,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--arenas", type=int, default=8192)
-    ap.add_argument("--team-size", type=int, default=0)
+    ap.add_argument("--team-size", type=int, default=2)
     ap.add_argument("--tick-skip", type=int, default=8)
-    ap.add_argument("--workload-name", default="soccar ball-only x 8192 arenas, tickSkip 8 (cars not built yet)")
+    ap.add_argument("--workload-name",
+                    default="soccar 2v2 x 8192 arenas, tickSkip 8, random-state starts, random discrete actions "
+                            "(physics step; obs/reward building not yet in the step)")
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

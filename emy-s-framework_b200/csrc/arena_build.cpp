@@ -271,6 +271,8 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
         Xf id = xfIdentity();
         V3 mn, mx;
         transformAabb(m.localMin, m.localMax, 0.f, id, mn, mx);
+        d.shapeMin = mn;
+        d.shapeMax = mx;
         V3 thr{0.02f, 0.02f, 0.02f};
         d.bpMin = mn - thr;
         d.bpMax = mx + thr;
@@ -377,6 +379,8 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
             mx[axis] = origins[p][axis] + (c + kOff);
             if (n[axis] < 0) mx[axis] = kLargeFloat;
             else mn[axis] = -kLargeFloat;
+            S.planeShapeMin[p] = mn;
+            S.planeShapeMax[p] = mx;
             V3 thr{0.02f, 0.02f, 0.02f};
             S.planeBpMin[p] = mn - thr;
             S.planeBpMax[p] = mx + thr;

@@ -51,6 +51,7 @@ struct MeshDesc {
     int32_t triOff, triCount;
     V3 bvhMin, bvhMax, quant;  // quantization frame (btQuantizedBvh m_bvhAabbMin/Max/Quantization)
     V3 bpMin, bpMax;           // broadphase AABB (shape AABB +- gContactBreakingThreshold)
+    V3 shapeMin, shapeMax;     // btTriangleMeshShape::getAabb at the identity transform
 };
 
 // btRSBroadphase grid (Arena.cpp:459-471 with ArenaConfig defaults)
@@ -73,6 +74,7 @@ struct ArenaStatic {
     V3 planeNormal[NUM_PLANES];
     V3 planeOrigin[NUM_PLANES];
     V3 planeBpMin[NUM_PLANES], planeBpMax[NUM_PLANES];
+    V3 planeShapeMin[NUM_PLANES], planeShapeMax[NUM_PLANES];  // btStaticPlaneShape::getAabb
 };
 
 // ------------------------------------------------------------ BVH queries (device)

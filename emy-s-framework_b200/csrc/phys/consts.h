@@ -98,40 +98,56 @@ RSB_HD float curveOut(const Curve& c, float input, float def = 1.f) {
     return c.y[c.n - 1];
 }
 
-constexpr Curve STEER_ANGLE_FROM_SPEED_CURVE = {6, {0, 500, 1000, 1500, 1750, 3000},
-                                                {0.53356f, 0.31930f, 0.18203f, 0.10570f, 0.08507f, 0.03454f}};
-constexpr Curve POWERSLIDE_STEER_ANGLE_FROM_SPEED_CURVE = {2, {0, 2500}, {0.39235f, 0.12610f}};
-constexpr Curve DRIVE_SPEED_TORQUE_FACTOR_CURVE = {3, {0, 1400, 1410}, {1.0f, 0.1f, 0.0f}};
-constexpr Curve NON_STICKY_FRICTION_FACTOR_CURVE = {3, {0, 0.7075f, 1}, {0.1f, 0.5f, 1.0f}};
-constexpr Curve LAT_FRICTION_CURVE = {2, {0, 1}, {1.0f, 0.2f}};
-constexpr Curve LONG_FRICTION_CURVE = {0, {}, {}};
-constexpr Curve HANDBRAKE_LAT_FRICTION_FACTOR_CURVE = {1, {0}, {0.1f}};
-constexpr Curve HANDBRAKE_LONG_FRICTION_FACTOR_CURVE = {2, {0, 1}, {0.5f, 0.9f}};
-constexpr Curve BALL_CAR_EXTRA_IMPULSE_FACTOR_CURVE = {4, {0, 500.f, 2300.f, 4600.f}, {0.65f, 0.65f, 0.55f, 0.30f}};
-constexpr Curve BUMP_VEL_AMOUNT_GROUND_CURVE = {3, {0.f, 1400.f, 2200.f}, {(5.f / 6.f), 1100.f, 1530.f}};
-constexpr Curve BUMP_VEL_AMOUNT_AIR_CURVE = {3, {0.f, 1400.f, 2200.f}, {(5.f / 6.f), 1390.f, 1945.f}};
-constexpr Curve BUMP_UPWARD_VEL_AMOUNT_CURVE = {3, {0.f, 1400.f, 2200.f}, {(2.f / 6.f), 278.f, 417.f}};
+// Curves are produced by value (functions usable from host and device code):
+// crvSteerAngle = STEER_ANGLE_FROM_SPEED_CURVE, crvPowerslideSteer =
+// POWERSLIDE_STEER_ANGLE_FROM_SPEED_CURVE, crvDriveTorque = DRIVE_SPEED_TORQUE_FACTOR_CURVE,
+// crvNonSticky = NON_STICKY_FRICTION_FACTOR_CURVE, crvLatFriction / crvLongFriction =
+// LAT_ / LONG_FRICTION_CURVE, crvHandbrakeLat / crvHandbrakeLong =
+// HANDBRAKE_LAT_ / HANDBRAKE_LONG_FRICTION_FACTOR_CURVE, crvBallCarExtra =
+// BALL_CAR_EXTRA_IMPULSE_FACTOR_CURVE, crvBumpGround / crvBumpAir / crvBumpUp =
+// BUMP_VEL_AMOUNT_GROUND_ / BUMP_VEL_AMOUNT_AIR_ / BUMP_UPWARD_VEL_AMOUNT_CURVE.
+#define RSB_CURVE(fn, ...) \
+    RSB_HD Curve fn() { return Curve __VA_ARGS__; }
+RSB_CURVE(crvSteerAngle, {6, {0, 500, 1000, 1500, 1750, 3000}, {0.53356f, 0.31930f, 0.18203f, 0.10570f, 0.08507f, 0.03454f}})
+RSB_CURVE(crvPowerslideSteer, {2, {0, 2500}, {0.39235f, 0.12610f}})
+RSB_CURVE(crvDriveTorque, {3, {0, 1400, 1410}, {1.0f, 0.1f, 0.0f}})
+RSB_CURVE(crvNonSticky, {3, {0, 0.7075f, 1}, {0.1f, 0.5f, 1.0f}})
+RSB_CURVE(crvLatFriction, {2, {0, 1}, {1.0f, 0.2f}})
+RSB_CURVE(crvLongFriction, {0, {}, {}})
+RSB_CURVE(crvHandbrakeLat, {1, {0}, {0.1f}})
+RSB_CURVE(crvHandbrakeLong, {2, {0, 1}, {0.5f, 0.9f}})
+RSB_CURVE(crvBallCarExtra, {4, {0, 500.f, 2300.f, 4600.f}, {0.65f, 0.65f, 0.55f, 0.30f}})
+RSB_CURVE(crvBumpGround, {3, {0.f, 1400.f, 2200.f}, {(5.f / 6.f), 1100.f, 1530.f}})
+RSB_CURVE(crvBumpAir, {3, {0.f, 1400.f, 2200.f}, {(5.f / 6.f), 1390.f, 1945.f}})
+RSB_CURVE(crvBumpUp, {3, {0.f, 1400.f, 2200.f}, {(2.f / 6.f), 278.f, 417.f}})
+#undef RSB_CURVE
 
 // Boost pad locations, big pads first (RLConst.h:222-252)
 struct PadLoc { float x, y, z; };
+#define RSB_PAD_LOCS                                                                     \
+    {{-3584.f, 0.f, 73.f}, {3584.f, 0.f, 73.f}, {-3072.f, 4096.f, 73.f},                 \
+     {3072.f, 4096.f, 73.f}, {-3072.f, -4096.f, 73.f}, {3072.f, -4096.f, 73.f},          \
+     {0.f, -4240.f, 70.f}, {-1792.f, -4184.f, 70.f}, {1792.f, -4184.f, 70.f},           \
+     {-940.f, -3308.f, 70.f}, {940.f, -3308.f, 70.f}, {0.f, -2816.f, 70.f},             \
+     {-3584.f, -2484.f, 70.f}, {3584.f, -2484.f, 70.f}, {-1788.f, -2300.f, 70.f},       \
+     {1788.f, -2300.f, 70.f}, {-2048.f, -1036.f, 70.f}, {0.f, -1024.f, 70.f},           \
+     {2048.f, -1036.f, 70.f}, {-1024.f, 0.f, 70.f}, {1024.f, 0.f, 70.f},                \
+     {-2048.f, 1036.f, 70.f}, {0.f, 1024.f, 70.f}, {2048.f, 1036.f, 70.f},              \
+     {-1788.f, 2300.f, 70.f}, {1788.f, 2300.f, 70.f}, {-3584.f, 2484.f, 70.f},          \
+     {3584.f, 2484.f, 70.f}, {0.f, 2816.f, 70.f}, {-940.f, 3308.f, 70.f},               \
+     {940.f, 3308.f, 70.f}, {-1792.f, 4184.f, 70.f}, {1792.f, 4184.f, 70.f},            \
+     {0.f, 4240.f, 70.f}}
+static constexpr PadLoc PAD_LOCS_HOST[NUM_PADS] = RSB_PAD_LOCS;
 #if defined(__CUDACC__)
-__device__ __constant__
-#else
-static
+__device__ __constant__ PadLoc PAD_LOCS_DEV[NUM_PADS] = RSB_PAD_LOCS;
 #endif
-const PadLoc PAD_LOCS[NUM_PADS] = {
-    {-3584.f, 0.f, 73.f}, {3584.f, 0.f, 73.f}, {-3072.f, 4096.f, 73.f},
-    {3072.f, 4096.f, 73.f}, {-3072.f, -4096.f, 73.f}, {3072.f, -4096.f, 73.f},
-    {0.f, -4240.f, 70.f}, {-1792.f, -4184.f, 70.f}, {1792.f, -4184.f, 70.f},
-    {-940.f, -3308.f, 70.f}, {940.f, -3308.f, 70.f}, {0.f, -2816.f, 70.f},
-    {-3584.f, -2484.f, 70.f}, {3584.f, -2484.f, 70.f}, {-1788.f, -2300.f, 70.f},
-    {1788.f, -2300.f, 70.f}, {-2048.f, -1036.f, 70.f}, {0.f, -1024.f, 70.f},
-    {2048.f, -1036.f, 70.f}, {-1024.f, 0.f, 70.f}, {1024.f, 0.f, 70.f},
-    {-2048.f, 1036.f, 70.f}, {0.f, 1024.f, 70.f}, {2048.f, 1036.f, 70.f},
-    {-1788.f, 2300.f, 70.f}, {1788.f, 2300.f, 70.f}, {-3584.f, 2484.f, 70.f},
-    {3584.f, 2484.f, 70.f}, {0.f, 2816.f, 70.f}, {-940.f, 3308.f, 70.f},
-    {940.f, 3308.f, 70.f}, {-1792.f, 4184.f, 70.f}, {1792.f, 4184.f, 70.f},
-    {0.f, 4240.f, 70.f}};
+RSB_HD PadLoc padLoc(int p) {
+#if defined(__CUDA_ARCH__)
+    return PAD_LOCS_DEV[p];
+#else
+    return PAD_LOCS_HOST[p];
+#endif
+}
 
 // Car spawn / respawn tables for blue (RLConst.h:278-311); orange is mirrored.
 struct SpawnPos { float x, y, yaw; };

@@ -22,16 +22,6 @@ struct BallP {
     uint32_t regStamp;
 };
 
-// CarState flag bits
-enum : uint32_t {
-    CF_ON_GROUND = 1u << 0, CF_HAS_JUMPED = 1u << 1, CF_HAS_DOUBLE_JUMPED = 1u << 2,
-    CF_HAS_FLIPPED = 1u << 3, CF_IS_FLIPPING = 1u << 4, CF_IS_JUMPING = 1u << 5,
-    CF_SUPERSONIC = 1u << 6, CF_AUTO_FLIPPING = 1u << 7, CF_DEMOED = 1u << 8,
-    CF_WORLD_CONTACT = 1u << 9, CF_BALL_HIT_VALID = 1u << 10,
-    CF_WHEEL0 = 1u << 11,  // 4 bits: wheelsWithContact
-    CF_TEAM_ORANGE = 1u << 15
-};
-
 struct CarP {
     float pos[3];
     float rot[9];
@@ -50,9 +40,8 @@ struct CarP {
     uint32_t ballHitTick[2];       // lo, hi
     uint32_t ballHitExtraTick[2];
     float ballHitRelPos[3], ballHitBallPos[3], ballHitExtraVel[3];
-    // controls of this tick and of the previous tick (CarControls)
-    float ctl[5];                  // throttle, steer, pitch, yaw, roll
-    uint32_t ctlBits;              // jump | boost<<1 | handbrake<<2
+    float rotMat[9];               // CarState::rotMat (differs from rot only while demoed)
+    // controls of the previous tick (CarState::lastControls)
     float lastCtl[5];
     uint32_t lastCtlBits;
     // btWheelInfoRL values carried from one tick to the next
@@ -73,7 +62,7 @@ struct ArenaP {
     int32_t goalTeam;     // -1, 0 blue scored, 1 orange scored (latched since the last reset)
     int32_t touchedMask;  // cars that touched the ball in the current env step
     float noTouchTimer;
-    int32_t pad_;
+    int32_t scored;       // ball past a goal line after the last tick (Arena::IsBallScored)
 };
 
 constexpr int W_BALL = sizeof(BallP) / 4;

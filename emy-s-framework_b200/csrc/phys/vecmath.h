@@ -75,10 +75,11 @@ RSB_HD V3 safeNormalized(V3 a) {
     if (l2 >= kEpsilon * kEpsilon) return bdiv(a, fsqrt(l2));
     return V3{1.f, 0.f, 0.f};
 }
-// RocketSim Vec::Normalized (true component division)
+// RocketSim Vec::Normalized (MathTypes.h:88-95): true component division, zero below
+// a length of FLT_EPSILON squared
 RSB_HD V3 rsNormalized(V3 a) {
     float l = length(a);
-    if (l > kEpsilon) return vdiv(a, l);
+    if (l > kEpsilon * kEpsilon) return vdiv(a, l);
     return v3zero();
 }
 RSB_HD int maxAxis(V3 a) { return a.x < a.y ? (a.y < a.z ? 2 : 1) : (a.x < a.z ? 2 : 0); }

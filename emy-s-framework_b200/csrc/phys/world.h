@@ -13,6 +13,9 @@
 #pragma once
 #include "contacts.h"
 #include "solver.h"
+#include "ray.h"
+#include "gjk.h"
+#include "boxbox.h"
 
 namespace rsb {
 
@@ -29,7 +32,16 @@ struct World {
     Manifold m[MAX_MANIFOLDS];
     BlockPool pool;
     uint32_t status;
+    // cars
+    int nc;
+    CarSim c[MAX_CARS];
+    uint64_t tick;          // Arena::tickCount at the start of this tick
+    V3 ballVelCache;        // Ball::_velocityImpulseCache
+    EpaWork* epa;           // EPA scratch (faces and support vertices)
 };
+
+// world status bits (per-arena status word)
+enum : uint32_t { WS_NONFINITE = 1u, WS_OVERFLOW = 2u, WS_BVH_OVERFLOW = 4u, WS_EPA_OVERFLOW = 16u };
 
 // ------------------------------------------------------------------ objects
 
@@ -72,9 +84,19 @@ RSB_HD void ballAabb(const WorldParams& P, const Xf& xf, V3& mn, V3& mx) {
     mx = xf.o + e;
 }
 
+// Car hitbox: a btCompoundShape holding one btBoxShape at the hitbox offset
+RSB_HD Xf carChildXf(const CarParams& C, const Xf& carXf) { return xfMul(carXf, Xf{m3identity(), C.childOff}); }
+// btCompoundShape::getAabb
+RSB_HD void carCompoundAabb(const CarParams& C, const Xf& xf, V3& mn, V3& mx) { transformAabb(C.cmpMin, C.cmpMax, 0.f, xf, mn, mx); }
+// btBoxShape::getAabb of the child at its world transform
+RSB_HD void carBoxAabb(const CarParams& C, const Xf& childXf, V3& mn, V3& mx) {
+    transformAabbHalf(C.boxHe, C.boxMargin, childXf, mn, mx);
+}
+RSB_HD ConvexShape carBoxShape(const CarParams& C) { return makeBox(C.boxHe, C.boxMargin); }
+
 RSB_HD void bodyShapeAabb(const World& W, int bi, const Xf& xf, V3& mn, V3& mx) {
     if (bi == 0) ballAabb(*W.P, xf, mn, mx);
-    else { mn = xf.o; mx = xf.o; }  // cars: filled in by the car module
+    else carCompoundAabb(W.P->car, xf, mn, mx);
 }
 
 RSB_HD void bpCellIndices(const BpGrid& g, V3 pos, int& i, int& j, int& k) {
@@ -349,8 +371,271 @@ RSB_HD void collideBallPlane(World& W, int plane, Manifold& man) {
     if (man.n) refreshContactPoints(man, rBall.xf, rPlane.xf);
 }
 
+// ------------------------------------------------------------------ contact callbacks
+
+RSB_HD bool carResponds(const World& W, int ci) { return !W.b[1 + ci].noResp; }
+
+// Arena::_BtCallback_OnCarWorldCollision (Arena.cpp:420-427)
+RSB_HD void onCarWorld(World& W, int ci, MPoint& cp) {
+    CarSim& c = W.c[ci];
+    c.flags |= CF_WORLD_CONTACT;
+    c.worldContactNormal = cp.normal;
+    cp.fric = W.P->car.worldFriction;
+    cp.rest = W.P->car.worldRestitution;
+}
+
+// Arena::_BtCallback_OnCarBallCollision (Arena.cpp:278-332)
+RSB_HD void onCarBall(World& W, int ci, MPoint& cp, bool ballIsBodyA) {
+    const CarParams& C = W.P->car;
+    CarSim& c = W.c[ci];
+    const Body& cb = W.b[1 + ci];
+    const Body& bb = W.b[0];
+    V3 carPos = cb.xf.o * kBtToUu, carVel = cb.lin * kBtToUu;
+    V3 ballPos = bb.xf.o * kBtToUu, ballVel = bb.lin * kBtToUu;
+    cp.fric = CARBALL_COLLISION_FRICTION;
+    cp.rest = CARBALL_COLLISION_RESTITUTION;
+    c.flags |= CF_BALL_HIT_VALID;
+    c.ballHitRelPos = (ballIsBodyA ? cp.localA : cp.localB) * kBtToUu;
+    c.ballHitTick = W.tick;
+    c.ballHitBallPos = ballPos;
+    c.ballHitExtraVel = v3zero();
+    if ((W.tick > c.ballHitExtraTick + 1) || (c.ballHitExtraTick > W.tick)) c.ballHitExtraTick = W.tick;
+    else return;
+    V3 carForward = c.rotMat.col(0);
+    V3 relPos = ballPos - carPos;
+    V3 relVel = ballVel - carVel;
+    float relSpeed = fmin_(length(relVel), BALL_CAR_EXTRA_IMPULSE_MAXDELTAVEL_UU);
+    if (relSpeed > 0) {
+        V3 hitDir = safeNormalized(relPos * V3{1, 1, BALL_CAR_EXTRA_IMPULSE_Z_SCALE});
+        V3 fwdAdj = (carForward * dot(hitDir, carForward)) * (1 - BALL_CAR_EXTRA_IMPULSE_FORWARD_SCALE);
+        hitDir = safeNormalized(hitDir - fwdAdj);
+        V3 addedVel = ((hitDir * relSpeed) * curveOut(crvBallCarExtra(), relSpeed)) * C.ballHitExtraScale;
+        c.ballHitExtraVel = addedVel;
+        W.ballVelCache = W.ballVelCache + addedVel * kUuToBt;
+    }
+}
+
+// Arena::_BtCallback_OnCarCarCollision (Arena.cpp:334-418); car1 is the manifold's body 0
+RSB_HD void onCarCar(World& W, int car1, int car2, MPoint& cp) {
+    const CarParams& C = W.P->car;
+    cp.fric = CARCAR_COLLISION_FRICTION;
+    cp.rest = CARCAR_COLLISION_RESTITUTION;
+    for (int i = 0; i < 2; i++) {
+        bool isSwapped = (i == 1);
+        if (isSwapped) { int t = car1; car1 = car2; car2 = t; }
+        CarSim& s1 = W.c[car1];
+        CarSim& s2 = W.c[car2];
+        if ((s1.flags & CF_DEMOED) || (s2.flags & CF_DEMOED)) return;
+        if ((s1.carContactOtherId == s2.id) && (s1.carContactCooldown > 0)) continue;
+        V3 pos1 = W.b[1 + car1].xf.o * kBtToUu, vel1 = W.b[1 + car1].lin * kBtToUu;
+        V3 pos2 = W.b[1 + car2].xf.o * kBtToUu, vel2 = W.b[1 + car2].lin * kBtToUu;
+        V3 deltaPos = pos2 - pos1;
+        if (dot(vel1, deltaPos) > 0) {
+            V3 velDir = rsNormalized(vel1);
+            V3 dirToOther = rsNormalized(deltaPos);
+            float speedTowards = dot(vel1, dirToOther);
+            float otherAway = dot(vel2, velDir);
+            if (speedTowards > otherAway) {
+                V3 localPoint = isSwapped ? cp.localB : cp.localA;
+                bool hitWithBumper = (localPoint.x * kBtToUu) > BUMP_MIN_FORWARD_DIST;
+                if (hitWithBumper) {
+                    bool isDemo;
+                    if (C.demoMode == 1) isDemo = true;
+                    else if (C.demoMode == 2) isDemo = false;
+                    else isDemo = (s1.flags & CF_SUPERSONIC) != 0;
+                    if (isDemo && !C.teamDemos) isDemo = s1.team != s2.team;
+                    if (isDemo) {
+                        s2.flags |= CF_DEMOED;
+                        s2.demoRespawnTimer = C.respawnDelay;
+                    } else {
+                        bool groundHit = (s2.flags & CF_ON_GROUND) != 0;
+                        float baseScale = curveOut(groundHit ? crvBumpGround() : crvBumpAir(), speedTowards);
+                        V3 hitUpDir = groundHit ? s2.rotMat.col(2) : V3{0, 0, 1};
+                        V3 bump = velDir * baseScale + (hitUpDir * curveOut(crvBumpUp(), speedTowards)) * C.bumpForceScale;
+                        s2.velCache = s2.velCache + bump * kUuToBt;
+                    }
+                    s1.carContactOtherId = s2.id;
+                    s1.carContactCooldown = C.bumpCooldown;
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ narrowphase: cars
+
+// Manifold bookkeeping of btCollisionDispatcher: getNewManifold appends, releaseManifold
+// swaps the released manifold with the last one (btCollisionDispatcher.cpp:70-130).
+RSB_HD int newManifold(World& W, int o0, int o1, float cbt) {
+    if (W.nm >= MAX_MANIFOLDS) {
+        W.status |= WS_OVERFLOW;
+        return -1;
+    }
+    Manifold& m = W.m[W.nm];
+    m.o0 = o0;
+    m.o1 = o1;
+    m.cbt = cbt;
+    m.n = 0;
+    m.pt = nullptr;
+    return W.nm++;
+}
+RSB_HD void releaseManifold(World& W, int idx) {
+    if (idx < 0) return;
+    int last = W.nm - 1;
+    if (idx != last) W.m[idx] = W.m[last];
+    W.nm--;
+}
+
+RSB_HD float sq(float x) { return x * x; }
+
+// Car box vs one arena mesh: the compound's child algorithm is btConvexConcaveCollisionAlgorithm
+// (btConvexConcaveCollisionAlgorithm.cpp:60-250), each overlapping triangle through
+// btConvexConvexAlgorithm's GJK (btConvexConvexAlgorithm.cpp:268-590).
+RSB_HD void collideBoxMesh(World& W, int mesh, int ci, const Xf& childXf, Manifold& man) {
+    const CarParams& C = W.P->car;
+    int carObj = OBJ_CAR0 + ci;
+    ObjRef rMesh = objRef(W, mesh), rCar = objRef(W, carObj);
+    ConvexShape box = carBoxShape(C);
+    V3 amn, amx;
+    carBoxAabb(C, childXf, amn, amx);
+    M3 invB = inverse(childXf.b);
+    float maxDist2 = sq((C.boxMargin + 0.f) + man.cbt);
+    bool responds = carResponds(W, ci);
+    bvhQueryAabb(*W.S, mesh, amn, amx, [&](int tri) {
+        V3 v[3];
+        triVerts(*W.S, mesh, tri, v);
+        if (!triAabbOverlap(v, amn, amx)) return true;
+        V3 tn = normalized(cross(v[1] - v[0], v[2] - v[0]));
+        for (int side = 0; side < 2; side++) {
+            V3 lp = supportVirtual(box, invB * tn);
+            V3 wp = xfPoint(childXf, lp);
+            float dist = dot(tn, v[0]) - dot(tn, wp);
+            if (dist > man.cbt + 0.f) return true;
+            tn *= -1.f;
+        }
+        ConvexShape triS = makeTri(v, 0.f);
+        GjkOut g = gjkPairDetector(W.epa, box, childXf, triS, xfIdentity(), maxDist2);
+        if (g.overflow) W.status |= WS_EPA_OVERFLOW;
+        if (g.has) {
+            int idx = addContact(man, W.pool, mesh, rMesh, carObj, rCar, g.normal, g.point, g.dist);
+            if (idx >= 0 && responds) {
+                MPoint& cp = man.pt[idx];
+                cp.index1 = tri;
+                onCarWorld(W, ci, cp);
+                adjustInternalEdge(cp, v, W.S->triInfo[W.S->meshes[mesh].triOff + tri]);
+            }
+        }
+        return true;
+    });
+    if (man.n) refreshContactPoints(man, rCar.xf, rMesh.xf);
+}
+
+// Car box vs a static plane: btConvexPlaneCollisionAlgorithm owning its manifold
+RSB_HD void collideBoxPlane(World& W, int plane, int ci, const Xf& childXf, Manifold& man) {
+    const CarParams& C = W.P->car;
+    int carObj = OBJ_CAR0 + ci;
+    ObjRef rPlane = objRef(W, plane), rCar = objRef(W, carObj);
+    ConvexShape box = carBoxShape(C);
+    V3 pn = W.S->planeNormal[plane - MAX_MESHES];
+    Xf planeInConvex = xfMul(xfInverse(childXf), rPlane.xf);
+    Xf convexInPlane = xfMul(xfInverse(rPlane.xf), childXf);
+    V3 vtx = supportVirtual(box, planeInConvex.b * (-pn));
+    V3 vip = xfPoint(convexInPlane, vtx);
+    float distance = dot(pn, vip) - 0.f;
+    if (distance < man.cbt + 0.f) {
+        V3 proj = vip - pn * distance;
+        V3 world = xfPoint(rPlane.xf, proj);
+        V3 nb = rPlane.xf.b * pn;
+        int idx = addContact(man, W.pool, plane, rPlane, carObj, rCar, nb, world, distance);
+        if (idx >= 0 && carResponds(W, ci)) onCarWorld(W, ci, man.pt[idx]);
+    }
+    if (man.n) refreshContactPoints(man, rCar.xf, rPlane.xf);
+}
+
+// (static, car) pair: swapped btCompoundCollisionAlgorithm (btCompoundCollisionAlgorithm.cpp:120-330).
+// The child algorithm is built with the pair's algorithm, so its manifold exists before
+// processing; it is destroyed again when the child's AABB misses the static shape's AABB.
+RSB_HD void collideCarStatic(World& W, int s, int ci) {
+    const CarParams& C = W.P->car;
+    int mi = newManifold(W, OBJ_CAR0 + ci, s, C.cbt);
+    if (mi < 0) return;
+    Xf childXf = carChildXf(C, W.b[1 + ci].xf);
+    V3 bmn, bmx, omn, omx;
+    carBoxAabb(C, childXf, bmn, bmx);
+    if (s < MAX_MESHES) { omn = W.S->meshes[s].shapeMin; omx = W.S->meshes[s].shapeMax; }
+    else { omn = W.S->planeShapeMin[s - MAX_MESHES]; omx = W.S->planeShapeMax[s - MAX_MESHES]; }
+    bool overlap = aabbOverlap(bmn, bmx, omn, omx);
+    if (overlap) {
+        if (s < MAX_MESHES) collideBoxMesh(W, s, ci, childXf, W.m[mi]);
+        else collideBoxPlane(W, s, ci, childXf, W.m[mi]);
+    } else {
+        releaseManifold(W, mi);
+    }
+}
+
+// (ball, car) pair: swapped compound over a btConvexConvexAlgorithm that creates its
+// manifold on first use
+RSB_HD void collideCarBall(World& W, int ci) {
+    const WorldParams& P = *W.P;
+    const CarParams& C = P.car;
+    int carObj = OBJ_CAR0 + ci;
+    Xf childXf = carChildXf(C, W.b[1 + ci].xf);
+    V3 bmn, bmx, smn, smx;
+    carBoxAabb(C, childXf, bmn, bmx);
+    ballAabb(P, W.b[0].xf, smn, smx);
+    if (!aabbOverlap(bmn, bmx, smn, smx)) return;
+    int mi = newManifold(W, carObj, OBJ_BALL, fmin_(C.cbt, P.ballCbt));
+    if (mi < 0) return;
+    Manifold& man = W.m[mi];
+    ObjRef rBall = objRef(W, OBJ_BALL), rCar = objRef(W, carObj);
+    ConvexShape box = carBoxShape(C), sph = makeSphere(P.ballRadius);
+    float maxDist2 = sq((C.boxMargin + P.ballMargin) + man.cbt);
+    GjkOut g = gjkPairDetector(W.epa, box, childXf, sph, W.b[0].xf, maxDist2);
+    if (g.overflow) W.status |= WS_EPA_OVERFLOW;
+    if (g.has) {
+        int idx = addContact(man, W.pool, OBJ_BALL, rBall, carObj, rCar, g.normal, g.point, g.dist);
+        if (idx >= 0 && carResponds(W, ci)) onCarBall(W, ci, man.pt[idx], false);
+    }
+    if (man.n) refreshContactPoints(man, rCar.xf, rBall.xf);
+}
+
+// (car a, car b), a < b: btCompoundCompoundCollisionAlgorithm without child trees falls back to
+// the compound algorithm (car a's box vs car b's compound), whose child is a swapped compound
+// (car b's box vs car a's box) over btBoxBoxCollisionAlgorithm.  The box-box manifold is built
+// with the pair's algorithm, with car b as its body 0.
+RSB_HD void collideCarCar(World& W, int ca, int cb) {
+    const CarParams& C = W.P->car;
+    int objA = OBJ_CAR0 + ca, objB = OBJ_CAR0 + cb;
+    int mi = newManifold(W, objB, objA, C.cbt);
+    if (mi < 0) return;
+    Xf xa = carChildXf(C, W.b[1 + ca].xf), xb = carChildXf(C, W.b[1 + cb].xf);
+    V3 aMn, aMx, cMn, cMx, bMn, bMx;
+    carBoxAabb(C, xa, aMn, aMx);
+    carCompoundAabb(C, W.b[1 + cb].xf, cMn, cMx);
+    bool outer = aabbOverlap(aMn, aMx, cMn, cMx);
+    bool inner = false;
+    if (outer) {
+        carBoxAabb(C, xb, bMn, bMx);
+        inner = aabbOverlap(bMn, bMx, aMn, aMx);
+        if (inner) {
+            Manifold& man = W.m[mi];
+            ObjRef rA = objRef(W, objA), rB = objRef(W, objB);
+            BoxContacts bc;
+            boxBoxContacts(xb, C.boxHeM, xa, C.boxHeM, bc);
+            bool responds = carResponds(W, ca) && carResponds(W, cb);
+            for (int k = 0; k < bc.n; k++) {
+                int idx = addContact(man, W.pool, objA, rA, objB, rB, bc.c[k].normalOnB, bc.c[k].point, bc.c[k].depth);
+                if (idx >= 0 && responds) onCarCar(W, cb, ca, man.pt[idx]);
+            }
+            if (man.n) refreshContactPoints(man, rB.xf, rA.xf);
+        }
+    }
+    if (!(outer && inner)) releaseManifold(W, mi);
+}
+
 // ------------------------------------------------------------------ dispatch
 
+// btCollisionDispatcher::dispatchAllCollisionPairs in pair order
 RSB_HD void dispatchPairs(World& W) {
     W.nm = 0;
     W.pool.n = 0;
@@ -358,19 +643,100 @@ RSB_HD void dispatchPairs(World& W) {
     for (int p = 0; p < W.np; p++) {
         int o0 = W.po0[p], o1 = W.po1[p];
         if (!objActive(W, o0) && !objActive(W, o1)) continue;  // needsCollision
-        if (o1 == OBJ_BALL && objIsStatic(o0)) {
-            if (W.nm >= MAX_MANIFOLDS) { W.status |= 2u; continue; }
-            Manifold& man = W.m[W.nm++];
-            man.o0 = OBJ_BALL;
-            man.o1 = o0;
-            man.cbt = W.P->ballCbt;
-            man.n = 0;
-            man.pt = nullptr;
-            if (o0 < MAX_MESHES) collideBallMesh(W, o0, man);
-            else collideBallPlane(W, o0, man);
+        if (o1 == OBJ_BALL) {
+            int mi = newManifold(W, OBJ_BALL, o0, W.P->ballCbt);
+            if (mi < 0) continue;
+            if (o0 < MAX_MESHES) collideBallMesh(W, o0, W.m[mi]);
+            else collideBallPlane(W, o0, W.m[mi]);
+        } else if (objIsStatic(o0)) {
+            collideCarStatic(W, o0, o1 - OBJ_CAR0);
+        } else if (o0 == OBJ_BALL) {
+            collideCarBall(W, o1 - OBJ_CAR0);
+        } else {
+            collideCarCar(W, o0 - OBJ_CAR0, o1 - OBJ_CAR0);
         }
-        // car pairs are handled by the car narrowphase (added with the vehicle module)
     }
+}
+
+// ------------------------------------------------------------------ wheel ray casts
+
+// btDefaultVehicleRaycaster::castRay (btDefaultVehicleRaycaster.cpp:32-53) over
+// btCollisionWorld::rayTest with ClosestRayResultCallback ignoring the casting chassis.
+// The broadphase hands over every object registered in the cell of the ray start
+// (btRSBroadphase::rayTest, btRSBroadphase.cpp:325-356): statics in registration order,
+// then dynamic bodies in registration order; objects are tested without AABB culling.
+// Returns the object hit, or -1 (also when the closest object has no contact response).
+RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, V3& hitNormal, float& hitFrac) {
+    const ArenaStatic& S = *W.S;
+    const WorldParams& P = *W.P;
+    RayHit hit;
+    hit.fraction = 1.f;
+    hit.obj = -1;
+    hit.normal = v3zero();
+    auto testObj = [&](int o) {
+        if (hit.fraction == 0.f) return;
+        if (o == ignoreObj) return;
+        if (o < MAX_MESHES) {
+            rayVsMesh(S, o, from, to, hit);
+        } else if (o < NUM_STATICS) {
+            rayVsPlane(S, o, from, to, hit);
+        } else {
+            int bi = o - OBJ_BALL;
+            const Body& b = W.b[bi];
+            ConvexShape sh;
+            Xf x;
+            if (bi == 0) {
+                sh = makeSphere(P.ballRadius);
+                x = b.xf;
+            } else {
+                sh = carBoxShape(P.car);
+                x = carChildXf(P.car, b.xf);
+            }
+            float frac;
+            V3 n;
+            if (subsimplexCast(from, to, sh, x, frac, n)) {
+                if (length2(n) > 0.0001f && frac < hit.fraction) {
+                    hit.fraction = frac;
+                    hit.obj = o;
+                    hit.normal = normalized(n);
+                }
+            }
+        }
+    };
+    const BpGrid& g = S.bp;
+    float cs2 = g.cellSize * g.cellSize;
+    if (dist2(from, to) < cs2) {
+        int i, j, k;
+        bpCellIndices(g, from, i, j, k);
+        int cell = i * g.cellsY * g.cellsZ + j * g.cellsZ + k;
+        uint32_t mask = S.bpCells[cell];
+        for (int s = 0; s < NUM_STATICS; s++)
+            if (mask & (1u << s)) testObj(s);
+        uint32_t last = 0;
+        bool first = true;
+        for (int it = 0; it < W.nb; it++) {
+            int pick = -1;
+            uint32_t best = 0xffffffffu;
+            for (int e = 0; e < W.nb; e++) {
+                if (!inRegNeighbourhood(W.b[e], i, j, k)) continue;
+                uint32_t st = W.b[e].regStamp;
+                if ((first || st > last) && st < best) { best = st; pick = e; }
+            }
+            if (pick < 0) break;
+            first = false;
+            last = best;
+            testObj(OBJ_BALL + pick);
+        }
+    } else {
+        for (int o = 0; o < OBJ_BALL + W.nb; o++) testObj(o);
+    }
+    if (hit.obj < 0) return -1;
+    if (!objIsStatic(hit.obj) && W.b[hit.obj - OBJ_BALL].noResp) return -1;
+    float s = 1.f - hit.fraction;
+    hitPoint = from * s + to * hit.fraction;
+    hitNormal = normalized(hit.normal);
+    hitFrac = hit.fraction;
+    return hit.obj;
 }
 
 // ------------------------------------------------------------------ islands

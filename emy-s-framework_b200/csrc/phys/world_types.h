@@ -99,6 +99,33 @@ constexpr int MAX_CONTACT_ROWS = 64;
 constexpr int MAX_FRICTION_ROWS = 64;
 constexpr int MAX_PAIRS = 64;
 
+// Car body, hitbox and wheel constants, evaluated once on the host with the reference's
+// operation order (Car::_BulletSetup, Car.cpp:195-277; btBoxShape, btCompoundShape,
+// btRigidBody::setMassProps / setGravity) plus the mutator values the car logic reads.
+struct CarParams {
+    V3 boxHe;            // btBoxShape implicit half extents (without margin)
+    float boxMargin;     // setSafeMargin result
+    V3 boxHeM;           // half extents with margin
+    V3 childOff;         // hitbox offset of the compound's only child
+    V3 cmpMin, cmpMax;   // btCompoundShape local AABB
+    float cbt;           // contact breaking threshold of the compound shape
+    float invMass, mass; // mass = 1 / invMass (btRigidBody::getMass)
+    V3 invInertiaLocal;
+    V3 grav;             // gravity force (acceleration * (1 / invMass))
+    V3 wheelConn[4];     // chassis connection points
+    float wheelRadius[4], susRest[4], susForceScale[4];
+    float susTravel;     // m_maxSuspensionTravelCm / 100
+    float rayLen[4];     // rest + travel + radius - SUSPENSION_SUBTRACTION
+    float pushThresh[4]; // rest + radius - SUSPENSION_SUBTRACTION
+    float dodgeDeadzone;
+    float flipZDamp;     // powf(1 - FLIP_Z_DAMP_120, dt / (1 / 120))
+    // mutator values (MutatorConfig)
+    float jumpAccel, jumpImmediateForce, boostAccelGround, boostAccelAir, boostUsedPerSecond;
+    float respawnDelay, bumpCooldown, padCooldownBig, padCooldownSmall, spawnBoost;
+    float ballHitExtraScale, bumpForceScale, worldFriction, worldRestitution;
+    int32_t unlimitedFlips, unlimitedDoubleJumps, demoMode, teamDemos;
+};
+
 struct WorldParams {
     float dt;                 // 1/120
     V3 gravity;               // Bullet units
@@ -114,6 +141,54 @@ struct WorldParams {
     float ballMaxSpeedBt;
     float goalBaseY;          // mutator goalBaseThresholdY (uu)
     float ballRadiusUu;
+    CarParams car;
+    int8_t padGrid[8 * 10];   // BoostPadGrid cells (x * 10 + y) -> pad index, -1 empty
+};
+
+// ------------------------------------------------------------------ cars in a tick
+
+// One wheel's btWheelInfoRL raycast and force values of the current tick.
+struct WheelTick {
+    V3 hardPoint, dirWS, axleWS;
+    V3 contactPoint, contactNormal;
+    V3 impulse;
+    M3 basis;              // m_worldTransform basis (steering applied)
+    float suspLen, relVel, clippedInv, susForce;
+    int32_t ground;        // collision object hit by the ray, -1 none
+    int32_t inContact, withWorld;
+};
+
+// Car::_internalState plus the btVehicleRL values that persist between ticks.
+struct CarSim {
+    float boost, timeSpentBoosting, jumpTime, flipTime, airTime, airTimeSinceJump;
+    float supersonicTime, handbrakeVal, autoFlipTimer, autoFlipTorqueScale;
+    float demoRespawnTimer, carContactCooldown;
+    V3 flipRelTorque, worldContactNormal;
+    uint32_t carContactOtherId;
+    uint32_t flags;        // CF_* bits
+    uint64_t ballHitTick, ballHitExtraTick;
+    V3 ballHitRelPos, ballHitBallPos, ballHitExtraVel;
+    M3 rotMat;             // CarState::rotMat (basis after the last post-tick update)
+    float ctl[5];          // throttle, steer, pitch, yaw, roll
+    uint32_t ctlBits;      // jump | boost << 1 | handbrake << 2
+    float lastCtl[5];
+    uint32_t lastCtlBits;
+    float steerAngle, engineForce, brake;
+    float latF[4], longF[4], extraPush[4];
+    V3 velCache;           // _velocityImpulseCache
+    int32_t team;          // 0 blue, 1 orange
+    uint32_t id;           // car id (1-based, creation order)
+    WheelTick w[4];
+};
+
+// CarSim flag bits (shared with the persistent record)
+enum : uint32_t {
+    CF_ON_GROUND = 1u << 0, CF_HAS_JUMPED = 1u << 1, CF_HAS_DOUBLE_JUMPED = 1u << 2,
+    CF_HAS_FLIPPED = 1u << 3, CF_IS_FLIPPING = 1u << 4, CF_IS_JUMPING = 1u << 5,
+    CF_SUPERSONIC = 1u << 6, CF_AUTO_FLIPPING = 1u << 7, CF_DEMOED = 1u << 8,
+    CF_WORLD_CONTACT = 1u << 9, CF_BALL_HIT_VALID = 1u << 10,
+    CF_WHEEL0 = 1u << 11,  // 4 bits: wheelsWithContact
+    CF_TEAM_ORANGE = 1u << 15
 };
 
 }  // namespace rsb

@@ -18,7 +18,7 @@
 
 #include "rsb.h"
 #include "arena_build.h"
-#include "phys/engine_core.h"
+#include "engine_host.h"
 
 using namespace rsb;
 
@@ -52,7 +52,7 @@ StaticCache& cache() {
     return c;
 }
 
-using EngineDev = EngineView;
+static_assert(sizeof(CtlRec) == sizeof(rsb_controls), "controls record layout");
 
 }  // namespace
 
@@ -61,6 +61,7 @@ struct rsb_handle {
     int N = 0;
     int numCars = 0;
     int maxCars = 0;
+    uint64_t seed = 0;
     std::vector<int32_t> teamSize, carOffset;
     std::shared_ptr<DevStatic> stat;
     WorldParams P{};
@@ -91,10 +92,12 @@ static rsb_status cudaFail(rsb_handle* h, const char* what, cudaError_t e) {
 
 // ------------------------------------------------------------------ kernels
 
-__global__ void __launch_bounds__(128) stepKernel(EngineDev D, int ticks) {
+__global__ void __launch_bounds__(128) stepKernel(EngineView D, int ticks) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= D.N) return;
     ArenaSim A;
+    EpaWork epa;
+    A.W.epa = &epa;
     stepArena(D, a, ticks, A);
 }
 
@@ -108,56 +111,6 @@ __global__ void expandActionsKernel(const int32_t* idx, const rsb_controls* lut,
 
 // ------------------------------------------------------------------ host helpers
 
-static void computeParams(const rsb_mutators& m, WorldParams& P) {
-    P = WorldParams{};
-    P.dt = 1.f / 120.f;
-    P.gravity = V3{m.gravity.x, m.gravity.y, m.gravity.z} * kUuToBt;
-    P.ballRadius = m.ball_radius * kUuToBt;
-    P.ballMargin = P.ballRadius;
-    P.ballAabbExt = P.ballMargin + 0.08f;
-    // btCollisionShape::getBoundingSphere adds 0.08 (a double literal) to the sphere radius
-    P.ballCbt = (float)((double)P.ballRadius + 0.08) * 0.02f;
-    P.ballInvMass = 1.f / m.ball_mass;
-    P.ballGrav = P.gravity * (1.f / P.ballInvMass);
-    float inert = 0.4f * m.ball_mass * P.ballMargin * P.ballMargin;
-    P.ballInvInertia = V3{1.f / inert, 1.f / inert, 1.f / inert};
-    float drag = m.ball_drag < 0.f ? 0.f : (m.ball_drag > 1.f ? 1.f : m.ball_drag);
-    P.ballLinDampFactor = powf(1.f - drag, P.dt);
-    P.ballFriction = m.ball_world_friction;
-    P.ballRestitution = m.ball_world_restitution;
-    P.ballMaxSpeedBt = m.ball_max_speed * kUuToBt;
-    P.goalBaseY = m.goal_base_threshold_y;
-    P.ballRadiusUu = m.ball_radius;
-}
-
-static void initialCell(const ArenaStatic& S, V3 mn, int32_t& cell, int32_t& ci, int32_t& cj, int32_t& ck) {
-    int i, j, k;
-    bpCellIndices(S.bp, mn, i, j, k);
-    ci = i; cj = j; ck = k;
-    cell = i * S.bp.cellsY * S.bp.cellsZ + j * S.bp.cellsZ + k;
-}
-
-static M3 basisFromRot(const rsb_rotmat& r) {
-    // RocketSim RotMat is column-major (forward, right, up are the basis columns)
-    return m3(r.forward.x, r.right.x, r.up.x, r.forward.y, r.right.y, r.up.y, r.forward.z, r.right.z, r.up.z);
-}
-static rsb_rotmat rotFromBasis(const float* rot) {
-    rsb_rotmat r;
-    r.forward = rsb_vec3{rot[0], rot[3], rot[6]};
-    r.right = rsb_vec3{rot[1], rot[4], rot[7]};
-    r.up = rsb_vec3{rot[2], rot[5], rot[8]};
-    return r;
-}
-
-template <class T>
-static void planesToHost(const std::vector<uint32_t>& planes, int stride, int idx, T& rec) {
-    loadPlanes(rec, planes.data(), idx, stride);
-}
-template <class T>
-static void hostToPlanes(std::vector<uint32_t>& planes, int stride, int idx, const T& rec) {
-    storePlanes(rec, planes.data(), idx, stride);
-}
-
 static rsb_status download(rsb_handle* h, const uint32_t* d, std::vector<uint32_t>& host, size_t words) {
     host.resize(words);
     RSB_CUDA(cudaMemcpyAsync(host.data(), d, words * 4, cudaMemcpyDeviceToHost, h->stream));
@@ -170,8 +123,8 @@ static rsb_status upload(rsb_handle* h, uint32_t* d, const std::vector<uint32_t>
     return RSB_OK;
 }
 
-static EngineDev devView(rsb_handle* h) {
-    EngineDev D;
+static EngineView devView(rsb_handle* h) {
+    EngineView D;
     D.S = h->stat->view;
     D.P = h->P;
     D.N = h->N;
@@ -181,7 +134,8 @@ static EngineDev devView(rsb_handle* h) {
     D.car = h->dCar;
     D.pad = h->dPad;
     D.arena = h->dArena;
-    D.controls = h->dControls;
+    D.controls = reinterpret_cast<const CtlRec*>(h->dControls);
+    D.seed = (uint32_t)(h->seed ^ (h->seed >> 32));
     return D;
 }
 
@@ -193,30 +147,7 @@ extern "C" {
 
 rsb_status rsb_default_mutators(rsb_mutators* m) {
     if (!m) return RSB_ERR_INVALID;
-    *m = rsb_mutators{};
-    m->gravity = rsb_vec3{0, 0, GRAVITY_Z};
-    m->car_mass = CAR_MASS_BT;
-    m->car_world_friction = CARWORLD_COLLISION_FRICTION;
-    m->car_world_restitution = CARWORLD_COLLISION_RESTITUTION;
-    m->ball_mass = BALL_MASS_BT;
-    m->ball_max_speed = BALL_MAX_SPEED;
-    m->ball_drag = BALL_DRAG;
-    m->ball_world_friction = BALL_FRICTION;
-    m->ball_world_restitution = BALL_RESTITUTION;
-    m->jump_accel = JUMP_ACCEL;
-    m->jump_immediate_force = JUMP_IMMEDIATE_FORCE;
-    m->boost_accel_ground = BOOST_ACCEL_GROUND;
-    m->boost_accel_air = BOOST_ACCEL_AIR;
-    m->boost_used_per_second = BOOST_USED_PER_SECOND;
-    m->respawn_delay = DEMO_RESPAWN_TIME;
-    m->bump_cooldown_time = BUMP_COOLDOWN_TIME;
-    m->boost_pad_cooldown_big = PAD_COOLDOWN_BIG;
-    m->boost_pad_cooldown_small = PAD_COOLDOWN_SMALL;
-    m->car_spawn_boost_amount = BOOST_SPAWN_AMOUNT;
-    m->ball_hit_extra_force_scale = 1.f;
-    m->bump_force_scale = 1.f;
-    m->ball_radius = BALL_COLLISION_RADIUS_SOCCAR;
-    m->goal_base_threshold_y = SOCCAR_GOAL_SCORE_BASE_THRESHOLD_Y;
+    defaultMutators(m);
     return RSB_OK;
 }
 
@@ -249,18 +180,24 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     h = hp.get();
     h->device = cfg->device;
     h->N = cfg->num_arenas;
+    h->seed = cfg->seed;
     h->carOffset.push_back(0);
     for (int a = 0; a < h->N; a++) {
         int ts = cfg->team_sizes ? cfg->team_sizes[a] : cfg->team_size;
         if (ts < 0 || ts > RSB_MAX_TEAM_SIZE) return fail(nullptr, RSB_ERR_INVALID, "team size must be 0..3");
-        if (ts > 0) return fail(nullptr, RSB_ERR_UNSUPPORTED, "cars are not built into this library yet");
         h->teamSize.push_back(ts);
         h->carOffset.push_back(h->carOffset.back() + 2 * ts);
         h->maxCars = std::max(h->maxCars, 2 * ts);
     }
     h->numCars = h->carOffset.back();
+    {
+        // every launch reads and writes each arena's records once and reads its controls
+        uint64_t words = 0;
+        for (int a = 0; a < h->N; a++) words += W_BALL + W_ARENA + NUM_PADS * W_PAD + 2 * h->teamSize[a] * W_CAR;
+        h->stats.state_bytes_per_step = 2 * 4 * words + (uint64_t)h->numCars * sizeof(rsb_controls) + 8 * (uint64_t)h->N;
+    }
     if (cfg->mutators) h->mut = *cfg->mutators;
-    else rsb_default_mutators(&h->mut);
+    else defaultMutators(&h->mut);
     computeParams(h->mut, h->P);
 
     // static arena data (host build shared across handles, device copy per device)
@@ -324,32 +261,13 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
         return fail(nullptr, RSB_ERR_NOMEM, "device allocation failed");
     cudaMemcpy(h->dTeamSize, h->teamSize.data(), N * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(h->dCarOffset, h->carOffset.data(), (N + 1) * 4, cudaMemcpyHostToDevice);
-
-    // initial state: RocketSim's Arena constructor (ball at rest at its kickoff height,
-    // active pads) with the broadphase cells of the creation transforms
     {
-        const ArenaStatic& S = h->stat->view;
-        std::vector<uint32_t> ball((size_t)W_BALL * N), arena((size_t)W_ARENA * N), pads((size_t)W_PAD * NUM_PADS * N);
-        BallP bp{};
-        Xf x{m3identity(), V3{0, 0, BALL_REST_Z} * kUuToBt};
-        xfToP(x, bp.pos, bp.rot);
-        V3 mn, mx;
-        Xf x0{m3identity(), V3{0, 0, h->P.ballRadius}};
-        ballAabb(h->P, x0, mn, mx);
-        initialCell(S, mn, bp.cell, bp.ci, bp.cj, bp.ck);
-        bp.regStamp = 0;
-        ArenaP ap{};
-        ap.goalTeam = -1;
-        PadP pp{};
-        pp.bits = 1;
-        for (size_t a = 0; a < N; a++) {
-            hostToPlanes(ball, (int)N, (int)a, bp);
-            hostToPlanes(arena, (int)N, (int)a, ap);
-            for (int p = 0; p < NUM_PADS; p++) hostToPlanes(pads, (int)(N * NUM_PADS), (int)(p * N + a), pp);
-        }
-        cudaMemcpy(h->dBall, ball.data(), ball.size() * 4, cudaMemcpyHostToDevice);
-        cudaMemcpy(h->dArena, arena.data(), arena.size() * 4, cudaMemcpyHostToDevice);
-        cudaMemcpy(h->dPad, pads.data(), pads.size() * 4, cudaMemcpyHostToDevice);
+        HostRecords R;
+        initRecords(h->stat->view, h->P, h->teamSize, R);
+        cudaMemcpy(h->dBall, R.ball.data(), R.ball.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->dCar, R.car.data(), R.car.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->dArena, R.arena.data(), R.arena.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->dPad, R.pad.data(), R.pad.size() * 4, cudaMemcpyHostToDevice);
     }
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(nullptr, RSB_ERR_CUDA, "initial upload failed");
     *out = hp.release();
@@ -387,7 +305,7 @@ rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
     if (!h || ticks < 0) return fail(h, RSB_ERR_INVALID, "bad tick count");
     if (ticks == 0) return RSB_OK;
     RSB_CUDA(cudaSetDevice(h->device));
-    EngineDev D = devView(h);
+    EngineView D = devView(h);
     int block = 128, grid = (h->N + block - 1) / block;
     stepKernel<<<grid, block, 0, pick(h, stream)>>>(D, ticks);
     RSB_CUDA(cudaGetLastError());
@@ -443,12 +361,8 @@ rsb_status rsb_get_balls(rsb_handle* h, rsb_ball_state* out, int32_t n) {
     if (st) return st;
     for (int a = 0; a < n; a++) {
         BallP p;
-        planesToHost(planes, h->N, a, p);
-        rsb_ball_state& o = out[a];
-        o.pos = rsb_vec3{p.pos[0] * kBtToUu, p.pos[1] * kBtToUu, p.pos[2] * kBtToUu};
-        o.rot = rotFromBasis(p.rot);
-        o.vel = rsb_vec3{p.lin[0] * kBtToUu, p.lin[1] * kBtToUu, p.lin[2] * kBtToUu};
-        o.ang_vel = rsb_vec3{p.ang[0], p.ang[1], p.ang[2]};
+        loadPlanes(p, planes.data(), a, h->N);
+        out[a] = ballStateOf(p);
     }
     return RSB_OK;
 }
@@ -458,28 +372,55 @@ rsb_status rsb_set_balls(rsb_handle* h, const rsb_ball_state* in, int32_t n) {
     std::vector<uint32_t> planes;
     rsb_status st = download(h, h->dBall, planes, (size_t)W_BALL * h->N);
     if (st) return st;
+    std::vector<uint32_t> arena;
+    st = download(h, h->dArena, arena, (size_t)W_ARENA * h->N);
+    if (st) return st;
     for (int a = 0; a < n; a++) {
         BallP p;
-        planesToHost(planes, h->N, a, p);
-        const rsb_ball_state& s = in[a];
-        Xf x{basisFromRot(s.rot), V3{s.pos.x, s.pos.y, s.pos.z} * kUuToBt};
-        xfToP(x, p.pos, p.rot);
-        V3 v = V3{s.vel.x, s.vel.y, s.vel.z} * kUuToBt;
-        p.lin[0] = v.x; p.lin[1] = v.y; p.lin[2] = v.z;
-        p.ang[0] = s.ang_vel.x; p.ang[1] = s.ang_vel.y; p.ang[2] = s.ang_vel.z;
-        hostToPlanes(planes, h->N, a, p);
+        loadPlanes(p, planes.data(), a, h->N);
+        applyBallState(p, in[a]);
+        storePlanes(p, planes.data(), a, h->N);
+        // keep the arena's goal-line flag in step with the new ball position
+        ArenaP ap;
+        loadPlanes(ap, arena.data(), a, h->N);
+        float y = p.pos[1] * kBtToUu;
+        ap.scored = fabsf(y) > (h->P.goalBaseY + h->P.ballRadiusUu) ? (p.pos[1] > 0 ? 1 : 2) : 0;
+        storePlanes(ap, arena.data(), a, h->N);
     }
+    st = upload(h, h->dArena, arena);
+    if (st) return st;
     return upload(h, h->dBall, planes);
 }
 
 rsb_status rsb_get_cars(rsb_handle* h, rsb_car_state* out, int32_t n) {
     if (!h || (n > 0 && !out) || n != h->numCars) return fail(h, RSB_ERR_INVALID, "car count must equal num_cars");
+    if (n == 0) return RSB_OK;
+    std::vector<uint32_t> planes;
+    rsb_status st = download(h, h->dCar, planes, (size_t)W_CAR * MAX_CARS * h->N);
+    if (st) return st;
+    for (int a = 0; a < h->N; a++)
+        for (int s = 0; s < 2 * h->teamSize[a]; s++) {
+            CarP p;
+            loadPlanes(p, planes.data(), s * h->N + a, MAX_CARS * h->N);
+            out[h->carOffset[a] + s] = carStateOf(p, (uint32_t)s + 1u);
+        }
     return RSB_OK;
 }
 
 rsb_status rsb_set_cars(rsb_handle* h, const rsb_car_state* in, int32_t n) {
     if (!h || (n > 0 && !in) || n != h->numCars) return fail(h, RSB_ERR_INVALID, "car count must equal num_cars");
-    return RSB_OK;
+    if (n == 0) return RSB_OK;
+    std::vector<uint32_t> planes;
+    rsb_status st = download(h, h->dCar, planes, (size_t)W_CAR * MAX_CARS * h->N);
+    if (st) return st;
+    for (int a = 0; a < h->N; a++)
+        for (int s = 0; s < 2 * h->teamSize[a]; s++) {
+            CarP p;
+            loadPlanes(p, planes.data(), s * h->N + a, MAX_CARS * h->N);
+            applyCarState(p, in[h->carOffset[a] + s]);
+            storePlanes(p, planes.data(), s * h->N + a, MAX_CARS * h->N);
+        }
+    return upload(h, h->dCar, planes);
 }
 
 rsb_status rsb_get_pads(rsb_handle* h, rsb_pad_state* out, int32_t n) {
@@ -490,7 +431,7 @@ rsb_status rsb_get_pads(rsb_handle* h, rsb_pad_state* out, int32_t n) {
     for (int a = 0; a < h->N; a++)
         for (int p = 0; p < NUM_PADS; p++) {
             PadP pp;
-            planesToHost(planes, h->N * NUM_PADS, p * h->N + a, pp);
+            loadPlanes(pp, planes.data(), p * h->N + a, h->N * NUM_PADS);
             rsb_pad_state& o = out[a * NUM_PADS + p];
             o = rsb_pad_state{};
             o.is_active = pp.bits & 1;
@@ -509,32 +450,26 @@ rsb_status rsb_set_pads(rsb_handle* h, const rsb_pad_state* in, int32_t n) {
             PadP pp;
             pp.cooldown = s.cooldown;
             pp.bits = (s.is_active ? 1u : 0u) | (s.prev_locked_car_id << 8);
-            hostToPlanes(planes, h->N * NUM_PADS, p * h->N + a, pp);
+            storePlanes(pp, planes.data(), p * h->N + a, h->N * NUM_PADS);
         }
     return upload(h, h->dPad, planes);
 }
 
 rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
     if (!h || !out || n != h->N) return fail(h, RSB_ERR_INVALID, "info count must equal num_arenas");
-    std::vector<uint32_t> planes, balls;
+    std::vector<uint32_t> planes;
     rsb_status st = download(h, h->dArena, planes, (size_t)W_ARENA * h->N);
-    if (st) return st;
-    st = download(h, h->dBall, balls, (size_t)W_BALL * h->N);
     if (st) return st;
     for (int a = 0; a < n; a++) {
         ArenaP ap;
-        planesToHost(planes, h->N, a, ap);
-        BallP bp;
-        planesToHost(balls, h->N, a, bp);
+        loadPlanes(ap, planes.data(), a, h->N);
         rsb_arena_info& o = out[a];
         o = rsb_arena_info{};
         o.tick_count = (uint64_t)ap.tick[0] | ((uint64_t)ap.tick[1] << 32);
         o.num_cars = 2 * h->teamSize[a];
         o.team_size = h->teamSize[a];
-        float y = bp.pos[1] * kBtToUu;
-        bool scored = fabsf(y) > (h->mut.goal_base_threshold_y + h->mut.ball_radius);
-        o.goal_scored = scored;
-        o.goal_team = scored ? (y > 0 ? 0 : 1) : -1;
+        o.goal_scored = ap.scored != 0;
+        o.goal_team = ap.scored == 1 ? 0 : (ap.scored == 2 ? 1 : -1);
         o.episode_ticks = ap.episodeTicks;
         o.status = ap.status;
     }
@@ -569,7 +504,10 @@ rsb_status rsb_reset_all(rsb_handle* h, uint64_t, int32_t) {
 rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t*, int32_t, uint64_t, int32_t) {
     return fail(h, RSB_ERR_UNSUPPORTED, "resets are not built into this library yet");
 }
-rsb_status rsb_default_action_lut(rsb_controls*, int32_t) { return RSB_ERR_UNSUPPORTED; }
+rsb_status rsb_default_action_lut(rsb_controls* out, int32_t cap) {
+    if (!out || cap < RSB_NUM_ACTIONS) return RSB_ERR_INVALID;
+    return defaultActionLut(out, cap) == RSB_NUM_ACTIONS ? RSB_OK : RSB_ERR_STATE;
+}
 rsb_status rsb_snapshot(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
 rsb_status rsb_build_obs(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
 rsb_status rsb_build_rewards_terminals(rsb_handle* h, int32_t, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }

@@ -123,7 +123,7 @@ class Config(C.Structure):
 class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "ticks_simulated", "narrowphase_queries", "culled_queries", "missed_contacts",
-        "solver_rows", "arenas_reverted", "status_bits_seen")]
+        "solver_rows", "arenas_reverted", "status_bits_seen", "state_bytes_per_step")]
 
 
 CAR_DTYPE = np.dtype(CarState)
@@ -205,6 +205,35 @@ def default_action_lut(lib: C.CDLL) -> np.ndarray:
     st = lib.rsb_default_action_lut(_ptr(lut), RSB_NUM_ACTIONS)
     if st != 0:
         raise RsbError(st, "rsb_default_action_lut failed")
+    return lut
+
+
+def default_action_table() -> np.ndarray:
+    """The collector's 90-entry discrete action table built in Python (same enumeration as
+    RLGymCPP DefaultAction.cpp:3-60), for callers that have no engine library loaded."""
+    rows = []
+    for throttle in (-1, 0, 1):
+        for steer in (-1, 0, 1):
+            for boost in (0, 1):
+                for handbrake in (0, 1):
+                    if boost == 1 and throttle != 1:
+                        continue
+                    rows.append((throttle, steer, 0, steer, 0, 0, boost, handbrake))
+    for pitch in (-1, 0, 1):
+        for yaw in (-1, 0, 1):
+            for roll in (-1, 0, 1):
+                for jump in (0, 1):
+                    for boost in (0, 1):
+                        if jump == 1 and yaw != 0:
+                            continue
+                        if pitch == roll == jump == 0:
+                            continue
+                        handbrake = int(jump == 1 and (pitch != 0 or yaw != 0 or roll != 0))
+                        rows.append((boost, yaw, pitch, yaw, roll, jump, boost, handbrake))
+    lut = np.zeros(len(rows), CONTROLS_DTYPE)
+    for i, r in enumerate(rows):
+        for f, v in zip(("throttle", "steer", "pitch", "yaw", "roll", "jump", "boost", "handbrake"), r):
+            lut[i][f] = v
     return lut
 
 

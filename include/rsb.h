@@ -167,7 +167,8 @@ enum {
     RSB_ARENA_NONFINITE = 1,       /* NaN/Inf appeared in the state; arena should be reset */
     RSB_ARENA_ROW_OVERFLOW = 2,    /* more solver rows than the fixed pool; extra contacts dropped */
     RSB_ARENA_BVH_OVERFLOW = 4,    /* BVH traversal stack overflowed; query fell back to a linear scan */
-    RSB_ARENA_CULL_MISS = 8        /* the learned culler skipped a query that had a contact */
+    RSB_ARENA_CULL_MISS = 8,       /* the learned culler skipped a query that had a contact */
+    RSB_ARENA_EPA_OVERFLOW = 16    /* EPA's horizon walk exceeded its fixed stack; contact dropped */
 };
 
 /* RocketSim MutatorConfig (Sim/MutatorConfig/MutatorConfig.h:16-70), soccar defaults when NULL. */
@@ -222,6 +223,9 @@ typedef struct rsb_stats {
     uint64_t solver_rows;           /* contact rows solved */
     uint64_t arenas_reverted;       /* arenas switched back to the exact path */
     uint64_t status_bits_seen;      /* OR of all rsb_arena_info.status bits */
+    uint64_t state_bytes_per_step;  /* persistent state one rsb_step launch reads + writes
+                                       (the step kernel's algorithmic HBM traffic); 0 on
+                                       CPU implementations */
 } rsb_stats;
 
 typedef struct rsb_handle rsb_handle;

@@ -417,6 +417,26 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
 
 rsb_status rsb_sync(rsb_handle* h) { return h ? RSB_OK : RSB_ERR_INVALID; }
 
+// Oracle-only helpers (not part of include/rsb.h).
+//
+// rsbref_car_order: the order in which the reference visits the cars of arena `a` on
+// every tick (Arena::_cars is an unordered_set of pointers, so the order follows the
+// heap addresses of this run).  Writes car slot indices (blue first, then orange).
+int32_t rsbref_car_order(rsb_handle* h, int32_t a, int32_t* order) {
+    if (!h || a < 0 || a >= (int32_t)h->arenas.size() || !order) return -1;
+    int k = 0;
+    for (Car* c : h->arenas[a]->GetCars()) {
+        for (size_t s = 0; s < h->cars[a].size(); s++)
+            if (h->cars[a][s] == c) order[k++] = (int32_t)s;
+    }
+    return k;
+}
+// rsbref_car_ptr: the reference Car object of slot s in arena a (debug probes)
+void* rsbref_car_ptr(rsb_handle* h, int32_t a, int32_t s) {
+    if (!h || a < 0 || a >= (int32_t)h->arenas.size() || s < 0 || s >= (int32_t)h->cars[a].size()) return nullptr;
+    return h->cars[a][s];
+}
+
 rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out) {
     if (!h || !out) return RSB_ERR_INVALID;
     *out = h->stats;

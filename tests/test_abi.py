@@ -3,6 +3,8 @@ include/rsb.h declares; the engine refuses to run without a CUDA device."""
 from __future__ import annotations
 
 import os
+
+import numpy as np
 import re
 
 import pytest
@@ -41,3 +43,24 @@ def test_oracle_rejects_bad_config(pkg, oracle_lib, meshes_dir):
         pkg.rsb.Batch(oracle_lib, 0, team_size=1, meshes_path=meshes_dir)
     with pytest.raises(pkg.rsb.RsbError):
         pkg.rsb.Batch(oracle_lib, 1, team_size=4, meshes_path=meshes_dir)
+
+
+def test_default_action_table_matches_engine(pkg):
+    """The 90-action table from the engine's C ABI equals the Python enumeration."""
+    rsb = pkg.rsb
+    a = rsb.default_action_lut(pkg.engine_library())
+    b = rsb.default_action_table()
+    assert len(a) == rsb.RSB_NUM_ACTIONS == len(b)
+    assert a.tobytes() == b.tobytes()
+
+
+def test_default_action_table_shape(pkg):
+    """24 ground actions first (no boost below full throttle), then 66 aerial ones."""
+    lut = pkg.rsb.default_action_table()
+    ground, air = lut[:24], lut[24:]
+    assert (ground["pitch"] == 0).all() and (ground["jump"] == 0).all()
+    assert (ground["yaw"] == ground["steer"]).all()
+    assert ((ground["boost"] == 0) | (ground["throttle"] == 1)).all()
+    assert (air["throttle"] == air["boost"]).all() and (air["steer"] == air["yaw"]).all()
+    assert not ((air["jump"] == 1) & (air["yaw"] != 0)).any()
+    assert len(np.unique(lut.tobytes())) == 1 and len({r.tobytes() for r in lut}) == 90

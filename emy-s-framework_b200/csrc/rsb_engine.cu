@@ -54,6 +54,22 @@ StaticCache& cache() {
 
 static_assert(sizeof(CtlRec) == sizeof(rsb_controls), "controls record layout");
 
+// Staging array of rsb_set_actions_host_static: part of the module image, so using it
+// allocates nothing.  Every call overwrites the first n entries before the expansion
+// kernel reads them; nothing needs to start at zero.
+__device__ __align__(256) int32_t g_staticActions[RSB_STATIC_ACTIONS_MAX];
+
+// Device address of g_staticActions, looked up once per device (cudaGetSymbolAddress
+// with that device current).
+struct StaticActionsAddr {
+    std::mutex mu;
+    std::map<int, int32_t*> ptr;
+};
+StaticActionsAddr& staticActionsAddr() {
+    static StaticActionsAddr s;
+    return s;
+}
+
 }  // namespace
 
 struct rsb_handle {
@@ -352,6 +368,32 @@ rsb_status rsb_set_actions_host(rsb_handle* h, const int32_t* idx, int32_t n) {
     if (n == 0) return RSB_OK;
     RSB_CUDA(cudaMemcpyAsync(h->dActions, idx, 4 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
     return rsb_set_actions_device(h, h->dActions, n, nullptr);
+}
+
+rsb_status rsb_set_actions_host_static(rsb_handle* h, const int32_t* idx, int32_t n) {
+    if (h && n > RSB_STATIC_ACTIONS_MAX)
+        return fail(h, RSB_ERR_INVALID, "rsb_set_actions_host_static: more than RSB_STATIC_ACTIONS_MAX actions");
+    if (!h || !idx || n != h->numCars) return fail(h, RSB_ERR_INVALID, "action count must equal num_cars");
+    if (!h->dLut) return fail(h, RSB_ERR_STATE, "no action table uploaded");
+    if (n == 0) return RSB_OK;
+    RSB_CUDA(cudaSetDevice(h->device));
+    int32_t* stage = nullptr;
+    {
+        StaticActionsAddr& s = staticActionsAddr();
+        std::lock_guard<std::mutex> lock(s.mu);
+        auto it = s.ptr.find(h->device);
+        if (it == s.ptr.end()) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_staticActions);
+            if (e != cudaSuccess) return cudaFail(h, "cudaGetSymbolAddress(g_staticActions)", e);
+            it = s.ptr.emplace(h->device, static_cast<int32_t*>(p)).first;
+        }
+        stage = it->second;
+    }
+    RSB_CUDA(cudaMemcpyAsync(stage, idx, 4 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+    expandActionsKernel<<<(n + 255) / 256, 256, 0, h->stream>>>(stage, h->dLut, h->lutCount, h->dControls, n);
+    RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
 }
 
 rsb_status rsb_get_balls(rsb_handle* h, rsb_ball_state* out, int32_t n) {

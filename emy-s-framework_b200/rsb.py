@@ -23,6 +23,7 @@ import numpy as np
 RSB_MAX_CARS_PER_ARENA = 6
 RSB_NUM_PADS = 34
 RSB_NUM_ACTIONS = 90
+RSB_STATIC_ACTIONS_MAX = 65536 * 6
 RSB_OBS_BASE = 51
 RSB_OBS_PER_CAR = 29
 
@@ -145,6 +146,7 @@ _SIGS = {
     "rsb_set_action_lut": [_P, _P, C.c_int32],
     "rsb_default_action_lut": [_P, C.c_int32],
     "rsb_set_actions_host": [_P, _P, C.c_int32],
+    "rsb_set_actions_host_static": [_P, _P, C.c_int32],
     "rsb_set_actions_device": [_P, _P, C.c_int32, _P],
     "rsb_set_controls": [_P, _P, C.c_int32],
     "rsb_step": [_P, C.c_int32, _P],
@@ -323,6 +325,12 @@ class Batch:
     def set_actions(self, idx):
         a = np.ascontiguousarray(idx, np.int32)
         self._check(self.lib.rsb_set_actions_host(self._h, _ptr(a), len(a)))
+
+    def set_actions_static(self, idx):
+        """rsb_set_actions_host_static: stages the indices in the library's static device
+        array (no allocation on this path; see include/rsb.h)."""
+        a = np.ascontiguousarray(idx, np.int32)
+        self._check(self.lib.rsb_set_actions_host_static(self._h, _ptr(a), len(a)))
 
     def set_actions_device(self, dev_ptr: int, n: int, stream: int | None = None):
         self._check(self.lib.rsb_set_actions_device(self._h, C.c_void_p(dev_ptr), n, C.c_void_p(stream or 0)))

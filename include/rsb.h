@@ -253,6 +253,17 @@ rsb_status rsb_set_action_lut(rsb_handle* h, const rsb_controls* lut, int32_t co
 rsb_status rsb_default_action_lut(rsb_controls* lut, int32_t count);
 rsb_status rsb_set_actions_host(rsb_handle* h, const int32_t* idx, int32_t n);
 rsb_status rsb_set_actions_device(rsb_handle* h, const int32_t* d_idx, int32_t n, void* stream);
+/* Same result as rsb_set_actions_host, for callers that must not allocate device memory
+ * on the calling path (e.g. a collector running inside a memory budget fixed before the
+ * first step): the host indices are staged in a statically sized device array that is
+ * part of the library image instead of a buffer allocated for the handle.  At most
+ * RSB_STATIC_ACTIONS_MAX indices per call (larger n returns RSB_ERR_INVALID).  The first
+ * call on a device looks up the array's address (no allocation); make that first call
+ * before capturing the handle's stream into a graph.  The array is shared by every handle
+ * on a device: calls from two handles of one device must not overlap in time.  No
+ * counterpart in the reference (RocketSimCuda.h has only the allocating variant). */
+#define RSB_STATIC_ACTIONS_MAX (65536 * 6)
+rsb_status rsb_set_actions_host_static(rsb_handle* h, const int32_t* idx, int32_t n);
 rsb_status rsb_set_controls(rsb_handle* h, const rsb_controls* controls, int32_t n);
 
 rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream);

@@ -285,6 +285,12 @@ rsb_status rsb_set_actions_host(rsb_handle* h, const int32_t* idx, int32_t n) {
     return RSB_OK;
 }
 
+// CPU implementation: no device staging exists, so this equals rsb_set_actions_host.
+rsb_status rsb_set_actions_host_static(rsb_handle* h, const int32_t* idx, int32_t n) {
+    if (n > RSB_STATIC_ACTIONS_MAX) return fail(h, RSB_ERR_INVALID, "more than RSB_STATIC_ACTIONS_MAX actions");
+    return rsb_set_actions_host(h, idx, n);
+}
+
 static void stepRange(rsb_handle* h, int a0, int a1, int ticks) {
     for (int a = a0; a < a1; a++) {
         auto& cars = h->cars[a];

@@ -1,10 +1,13 @@
 """Throughput benchmark: arena-ticks/s of the batched soccar simulator on B200.
 
-One step = one env step of every arena: actions in, `tick_skip` physics ticks, state
-out.  Timing follows the measurement contract: W untimed warm-up steps, then K steps,
-each bracketed by CUDA events on the stream the kernels run on, the L2 flushed
+One step = one env step of every arena, as the collector runs it: discrete actions in,
+`tick_skip` physics ticks, AdvancedObs rows + action masks, the four stub rewards and the
+terminal flags (goal, or 1,800 ticks since the reset), then the finished arenas reset to
+random states.  Timing follows the measurement contract: W untimed warm-up steps, then K
+steps, each bracketed by CUDA events on the stream the kernels run on, the L2 flushed
 (256 MB write) between timed steps, max over ranks.  `--impl reference` times the
-reference's own CPU RocketSim (oracle/_ref) on the host cores instead.
+reference's own CPU implementation (RocketSim + RLGymCPP's env pieces, oracle/_ref) on the
+host cores instead.
 """
 from __future__ import annotations
 
@@ -24,6 +27,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "emy-s-framework_b200")
 ORACLE_LIB = os.path.join(ROOT, "oracle", "_ref", "librsref.so")
 METRIC = "arena-ticks/s on 1 B200, learned-cull vs exact-BVH path; % of HBM roofline"
+EPISODE_TICKS = 1800
 
 
 def load_pkg():
@@ -99,9 +103,9 @@ class ClockSampler:
 # ------------------------------------------------------------------ workload
 
 class Workload:
-    """The timed configuration: soccar arenas at seeded random states (cars on the ground,
-    random headings / speeds / boost, ball anywhere), a fresh discrete action per car from
-    the 90-entry table every env step."""
+    """The timed configuration: soccar arenas started from seeded random states (RLGymCPP
+    RandomState distribution), a fresh discrete action per car from the 90-entry table every
+    env step, finished episodes reset to random states."""
 
     def __init__(self, args):
         self.num_arenas = args.arenas
@@ -113,43 +117,10 @@ class Workload:
         return {"workload": self.name, "arenas": self.num_arenas, "team_size": self.team_size,
                 "tick_skip": self.tick_skip, "narrowphase": "exact-bvh", "state": "fp32",
                 "actions": "uniform over the 90-action table, new each env step",
+                "obs": f"AdvancedObs {51 + 29 * 2 * self.team_size} floats + 90 masks per player",
+                "rewards": "Goal, TouchBall, VelocityBallToGoal, VelocityPlayerToBall",
+                "terminals": f"goal or {EPISODE_TICKS} ticks; finished arenas reset to random states",
                 "l2": "flushed between timed steps (256 MB write)"}
-
-
-def initial_cars(cars, seed):
-    rng = np.random.default_rng(seed)
-    c = cars.copy()
-    n = len(c)
-    yaw = rng.uniform(-np.pi, np.pi, n)
-    cy, sy = np.cos(yaw), np.sin(yaw)
-    c["pos"]["x"] = rng.uniform(-3500, 3500, n)
-    c["pos"]["y"] = rng.uniform(-4500, 4500, n)
-    c["pos"]["z"] = 17.0
-    c["rot"]["forward"]["x"], c["rot"]["forward"]["y"], c["rot"]["forward"]["z"] = cy, sy, 0
-    c["rot"]["right"]["x"], c["rot"]["right"]["y"], c["rot"]["right"]["z"] = -sy, cy, 0
-    c["rot"]["up"]["x"], c["rot"]["up"]["y"], c["rot"]["up"]["z"] = 0, 0, 1
-    sp = rng.uniform(0, 2300, n)
-    c["vel"]["x"], c["vel"]["y"], c["vel"]["z"] = cy * sp, sy * sp, 0
-    c["boost"] = rng.uniform(0, 100, n)
-    c["is_on_ground"] = 1
-    return c
-
-
-def initial_balls(rsb, n, seed):
-    rng = np.random.default_rng(seed)
-    b = np.zeros(n, rsb.BALL_DTYPE)
-    for k, f in enumerate(("forward", "right", "up")):
-        for c in "xyz":
-            b["rot"][f][c] = 1.0 if "xyz"[k] == c else 0.0
-    b["pos"]["x"] = rng.uniform(-3500, 3500, n)
-    b["pos"]["y"] = rng.uniform(-4000, 4000, n)
-    b["pos"]["z"] = rng.uniform(100, 1820, n)
-    sp = rng.uniform(0, 3000, n)
-    d = rng.normal(size=(n, 3))
-    d /= np.linalg.norm(d, axis=1, keepdims=True)
-    for k, c in enumerate("xyz"):
-        b["vel"][c] = d[:, k] * sp
-    return b
 
 
 # ------------------------------------------------------------------ our arm
@@ -162,11 +133,10 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     wl = Workload(args)
+    rewards = rsb.default_rewards(pkg.engine_library(), episode_max_ticks=EPISODE_TICKS)
     batch = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size,
-                      meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank)
-    batch.set_balls(initial_balls(rsb, wl.num_arenas, 0x5EED0001 + rank))
-    if batch.num_cars:
-        batch.set_cars(initial_cars(batch.get_cars(), 0x5EED0002 + rank))
+                      meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank, rewards=rewards)
+    batch.reset_all(0x5EED0001 + rank, rsb.RSB_RESET_RANDOM_STATE)
     batch.set_action_lut(rsb.default_action_lut(batch.lib))
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
@@ -175,13 +145,22 @@ def run_ours(args, rank, world, dist):
     gen.manual_seed(0x5EED0003 + rank)
     n_cars = max(1, batch.num_cars)
     actions = torch.empty(n_cars, dtype=torch.int32, device=dev)
+    counter = [0]
 
-    def one_step():
-        # the policy's actions arrive on the device; expand them and run tick_skip ticks
-        if batch.num_cars:
-            actions.random_(0, rsb.RSB_NUM_ACTIONS, generator=gen)
-            batch.set_actions_device(actions.data_ptr(), batch.num_cars, stream=sp)
+    def one_step(ev=None):
+        # the policy's actions arrive on the device; the whole env step stays there
+        actions.random_(0, rsb.RSB_NUM_ACTIONS, generator=gen)
+        batch.snapshot(stream=sp)
+        batch.set_actions_device(actions.data_ptr(), batch.num_cars, stream=sp)
+        if ev is not None:
+            ev[0].record(stream)
         batch.step(wl.tick_skip, stream=sp)
+        if ev is not None:
+            ev[1].record(stream)
+        batch.build_obs(stream=sp)
+        batch.build_rewards_terminals(wl.tick_skip, stream=sp)
+        counter[0] += 1
+        batch.reset_done(0x5EED1000 + counter[0], rsb.RSB_RESET_RANDOM_STATE, stream=sp)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -189,18 +168,20 @@ def run_ours(args, rank, world, dist):
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    times = []
+    times, step_times = [], []
     with ClockSampler(dev) as clocks, torch.cuda.stream(stream):
         torch.cuda.synchronize()
         for _ in range(args.steps):
             flush.fill_(1.0)  # evict the L2 between timed steps
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             e0.record(stream)
-            one_step()
+            one_step(ev)
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
+            step_times.append(ev[0].elapsed_time(ev[1]))
         torch.cuda.synchronize()
     total_ms = float(sum(times))
     if dist is not None:
@@ -211,26 +192,32 @@ def run_ours(args, rank, world, dist):
     arena_ticks = wl.num_arenas * wl.tick_skip * args.steps * world
     value = arena_ticks / (total_ms / 1e3)
 
-    # e2e through the public API with host buffers: host actions in (H2D), step, host read
-    # of the arena infos (D2H)
-    e2e_times = []
-    infos_bytes = wl.num_arenas * 32  # rsb_get_arena_info copies the 8-word arena record per arena
+    # e2e through the public API with host buffers, as the collector's host path runs it:
+    # host actions in (H2D), step, obs / masks / rewards / terminals back to the host (D2H),
+    # then the finished arenas reset by index (H2D of the index list)
+    e2e_times, h2d, d2h = [], [], []
     rng = np.random.default_rng(0x5EED0004 + rank)
     host_actions = rng.integers(0, rsb.RSB_NUM_ACTIONS, (16, n_cars)).astype(np.int32)
     for k in range(max(3, min(args.steps, 10))):
         t0 = time.perf_counter()
-        if batch.num_cars:
-            batch.set_actions(host_actions[k % 16, :batch.num_cars])
+        batch.snapshot()
+        batch.set_actions(host_actions[k % 16, :batch.num_cars])
         batch.step(wl.tick_skip)
-        batch.get_arena_info()
+        batch.build_obs()
+        batch.build_rewards_terminals(wl.tick_skip)
+        obs, masks, rew, term = batch.copy_obs(), batch.copy_masks(), batch.copy_rewards(), batch.copy_terminals()
+        done = np.nonzero(term)[0].astype(np.int32)
+        if done.size:
+            batch.reset_arenas(done, 0x5EED2000 + k, rsb.RSB_RESET_RANDOM_STATE)
         e2e_times.append(time.perf_counter() - t0)
+        h2d.append(4 * batch.num_cars + 4 * done.size)
+        d2h.append(obs.nbytes + masks.nbytes + rew.nbytes + term.nbytes)
     e2e_value = wl.num_arenas * wl.tick_skip * world / statistics.median(e2e_times)
-    h2d_bytes = 4 * batch.num_cars
 
-    # roofline of the step kernel: algorithmic bytes = persistent state read + written
-    # per launch (the library reports it)
+    # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
+    # state read + written per launch (the library reports it), over the kernel's own time
     alg_bytes = batch.stats()["state_bytes_per_step"]
-    kernel_s = (total_ms / args.steps) / 1e3
+    kernel_s = statistics.mean(step_times) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / kernel_s / 1e9
     res = {
@@ -238,12 +225,14 @@ def run_ours(args, rank, world, dist):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random states)",
         "config": wl.config() | {"parallelism": f"arena-shards x{world}"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "stepKernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                     "bytes_per_launch": alg_bytes},
-        "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": h2d_bytes,
-                "d2h_bytes_per_step": infos_bytes},
-        "gpu_launches": args.steps * (2 if batch.num_cars else 1),
+                     "bytes_per_launch": alg_bytes, "kernel_ms": kernel_s * 1e3,
+                     "kernel_share": statistics.mean(step_times) / (total_ms / args.steps)},
+        "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": int(statistics.mean(h2d)),
+                "d2h_bytes_per_step": int(statistics.mean(d2h))},
+        # per env step: action expansion, step, obs + masks, rewards + terminals, reset
+        "gpu_launches": args.steps * 5,
         "clocks": clocks.summary(),
     }
     return res
@@ -252,24 +241,28 @@ def run_ours(args, rank, world, dist):
 # ------------------------------------------------------------------ CPU reference
 
 def cpu_reference(args, sample_s=10.0, threads=None):
+    """The reference's CPU path for the same env step: RocketSim arenas stepped on all host
+    threads, then RLGymCPP's GameState / AdvancedObs / DefaultAction masks / stub rewards /
+    terminal conditions, then the finished arenas reset to random states."""
     pkg = load_pkg()
     rsb = pkg.rsb
     lib = rsb.load_library(ORACLE_LIB)
     threads = threads or os.cpu_count() or 1
     n = min(args.arenas, 64 * threads)
     wl = Workload(args)
-    b = rsb.Batch(lib, n, team_size=wl.team_size, meshes_path=pkg.MESHES_DIR, threads=threads)
-    b.set_balls(initial_balls(rsb, n, 0x5EED0001))
-    if b.num_cars:
-        b.set_cars(initial_cars(b.get_cars(), 0x5EED0002))
-    lut = rsb.default_action_table()
+    b = rsb.Batch(lib, n, team_size=wl.team_size, meshes_path=pkg.MESHES_DIR, threads=threads,
+                  rewards=rsb.default_rewards(lib, episode_max_ticks=EPISODE_TICKS))
+    b.reset_all(0x5EED0001, rsb.RSB_RESET_RANDOM_STATE)
+    b.set_action_lut(rsb.default_action_lut(lib))
     rng = np.random.default_rng(0x5EED0003)
-    pool = [lut[rng.integers(0, len(lut), max(1, b.num_cars))] for _ in range(16)]
+    pool = [rng.integers(0, rsb.RSB_NUM_ACTIONS, max(1, b.num_cars)).astype(np.int32) for _ in range(16)]
 
     def env_step(k):
-        if b.num_cars:
-            b.set_controls(pool[k % 16])
+        b.set_actions(pool[k % 16][:b.num_cars])
         b.step(wl.tick_skip)
+        b.build_obs()
+        b.build_rewards_terminals(wl.tick_skip)
+        b.reset_done(k, rsb.RSB_RESET_RANDOM_STATE)
 
     env_step(0)
     steps, t0 = 0, time.perf_counter()
@@ -278,7 +271,8 @@ def cpu_reference(args, sample_s=10.0, threads=None):
         steps += 1
     dt = time.perf_counter() - t0
     return {"value": n * wl.tick_skip * steps / dt, "unit": "arena-ticks/s", "cores": threads,
-            "kind": "reference", "sample": f"{n} arenas x {steps} env steps of {wl.tick_skip} ticks ({dt:.1f} s)"}
+            "kind": "reference", "sample": f"{n} arenas x {steps} env steps of {wl.tick_skip} ticks "
+                                          f"incl. obs/masks/rewards/terminals/resets ({dt:.1f} s)"}
 
 
 def run_reference(args):
@@ -301,8 +295,8 @@ def main():
     ap.add_argument("--team-size", type=int, default=2)
     ap.add_argument("--tick-skip", type=int, default=8)
     ap.add_argument("--workload-name",
-                    default="soccar 2v2 x 8192 arenas, tickSkip 8, random-state starts, random discrete actions "
-                            "(physics step; obs/reward building not yet in the step)")
+                    default="soccar 2v2 x 8192 arenas, tickSkip 8: random discrete actions -> 8 ticks -> "
+                            "AdvancedObs + masks -> 4 stub rewards + terminals -> random-state resets")
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

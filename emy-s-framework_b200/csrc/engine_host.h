@@ -204,6 +204,64 @@ inline void basisToFloats(const M3& b, float* rot) {
     }
 }
 
+// RLGymCPP's boost-pad order (CommonValues.h:48-84), used by its GameState and obs.
+constexpr float RLGYM_PAD_XY[NUM_PADS][2] = {
+    {0.f, -4240.f}, {-1792.f, -4184.f}, {1792.f, -4184.f}, {-3072.f, -4096.f}, {3072.f, -4096.f},
+    {-940.f, -3308.f}, {940.f, -3308.f}, {0.f, -2816.f}, {-3584.f, -2484.f}, {3584.f, -2484.f},
+    {-1788.f, -2300.f}, {1788.f, -2300.f}, {-2048.f, -1036.f}, {0.f, -1024.f}, {2048.f, -1036.f},
+    {-3584.f, 0.f}, {-1024.f, 0.f}, {1024.f, 0.f}, {3584.f, 0.f}, {-2048.f, 1036.f},
+    {0.f, 1024.f}, {2048.f, 1036.f}, {-1788.f, 2300.f}, {1788.f, 2300.f}, {-3584.f, 2484.f},
+    {3584.f, 2484.f}, {0.f, 2816.f}, {-940.f, 3310.f}, {940.f, 3308.f}, {-3072.f, 4096.f},
+    {3072.f, 4096.f}, {-1792.f, 4184.f}, {1792.f, 4184.f}, {0.f, 4240.f}};
+
+// Kickoff spawns of blue (RLConst.h:297-303: x, y, yaw as float).
+constexpr double kPi_d = 3.14159265358979323846;
+
+// Tables of the env kernels: the pad-order map of _BuildBoostPadIndexMap
+// (GameState.cpp:10-47, a 2D match within sqrt(10) uu), DefaultAction's four masks
+// (DefaultAction.cpp:62-90, over the default 90-entry table), and the kickoff bases
+// Angle(yaw, 0, 0).ToRotMat() with the orange yaw computed as `yaw += M_PI` on a float.
+// Returns false when a pad cannot be matched.
+template <class Tables>
+inline bool buildEnvTables(Tables& T) {
+    T = Tables{};
+    for (int i = 0; i < NUM_PADS; i++) {
+        int found = -1;
+        for (int j = 0; j < NUM_PADS && found < 0; j++) {
+            float dx = PAD_LOCS_HOST[j].x - RLGYM_PAD_XY[i][0], dy = PAD_LOCS_HOST[j].y - RLGYM_PAD_XY[i][1];
+            if (dx * dx + dy * dy < 10) found = j;
+        }
+        if (found < 0) return false;
+        T.padMap[i] = found;
+    }
+    rsb_controls lut[RSB_NUM_ACTIONS];
+    int n = defaultActionLut(lut, RSB_NUM_ACTIONS);
+    const int numGround = 24;
+    for (int i = 0; i < n; i++) {
+        const rsb_controls& c = lut[i];
+        auto set = [&](uint32_t* m) { m[i >> 5] |= 1u << (i & 31); };
+        if (c.jump) set(T.jump);
+        if (c.boost) set(T.boost);
+        if (i < numGround) set(T.ground);
+        if (i > numGround && !c.jump) set(T.air);
+        if (i < numGround && c.throttle == (float)c.boost && (float)(c.yaw != 0) == (float)c.handbrake) set(T.air);
+    }
+    const float yawBlue[NUM_KICKOFF_SPAWNS] = {(float)(kPi_d / 4 * 1), (float)(kPi_d / 4 * 3), (float)(kPi_d / 4 * 2),
+                                               (float)(kPi_d / 4 * 2), (float)(kPi_d / 4 * 2)};
+    const float xs[NUM_KICKOFF_SPAWNS] = {-2048, 2048, -256, 256, 0}, ys[NUM_KICKOFF_SPAWNS] = {-2560, -2560, -3840, -3840, -4608};
+    for (int k = 0; k < NUM_KICKOFF_SPAWNS; k++) {
+        T.kickX[k] = xs[k];
+        T.kickY[k] = ys[k];
+        for (int team = 0; team < 2; team++) {
+            float yaw = yawBlue[k];
+            if (team) yaw = (float)((double)yaw + kPi_d);
+            M3 r = m3fromEulerZYX(-0.f, -0.f, yaw);
+            basisToFloats(r, T.kickRot[team][k]);
+        }
+    }
+    return true;
+}
+
 // Records of a freshly created arena (Arena::Arena + Arena::AddCar): ball at rest at the
 // kickoff height, cars placed at respawn locations, pads active, and the broadphase
 // registrations of the creation transforms (ball first, then cars in creation order).

@@ -1,0 +1,558 @@
+// Env layer of the collector's GPU path, on the device: what GigaLearnCPP's EnvSet does
+// around each arena step, for every arena of the batch at once.
+//
+//   obsKernel ...... AdvancedObs rows and DefaultAction masks of every player
+//                    (RLGymCPP AdvancedObs.cpp:4-65, StateUtil.cpp:3-17 InvertPhys,
+//                    GameState.cpp:96-116 boost-pad order, DefaultAction.cpp:94-118)
+//   rewardKernel ... the four stub rewards and the terminal conditions of one env step
+//                    (CommonRewards.h:33-98, ZeroSumReward.cpp:3-31, GoalScoreCondition.h,
+//                    NoTouchCondition.h, EnvSet.cpp:184-254)
+//   resetKernel .... seeded arena resets: kickoff (Arena::ResetToRandomKickoff
+//                    Arena.cpp:112-216), random state (RandomState.cpp:9-60), high-contact
+//
+// Player order.  EnvSet walks the players of an arena in Arena::_cars order, which the
+// physics kernel takes to be reverse creation order (the order libstdc++'s unordered_set
+// visits the cars when each pointer hashes to its own bucket).  Observation rows and
+// reward slots are indexed by creation slot (the C ABI's packed player order), but the
+// teammate / opponent blocks inside a row, and the team sums of ZeroSumReward, follow the
+// reverse-slot order, as the reference's loops do.
+//
+// Floating point follows the reference expression by expression (RocketSim Vec: dot
+// products add a fourth "w" product, which is +0 here; divisions are IEEE divisions).
+#pragma once
+#include <stddef.h>
+
+#include "phys/state.h"
+#include "phys/engine_core.h"
+
+namespace rsb {
+
+// AdvancedObs coefficients (AdvancedObs.h:10-13)
+constexpr float OBS_POS = 1 / 5000.f, OBS_VEL = 1 / 2300.f, OBS_ANG = 1 / 3.f;
+// CommonValues.h:17-45
+constexpr float CV_BACK_NET_Y = 6000.f, CV_GOAL_HEIGHT = 642.775f, CV_BALL_MAX_SPEED = 6000.f,
+                CV_CAR_MAX_SPEED = 2300.f, CV_BALL_RADIUS = 92.75f;
+
+// Per-launch constant tables, built on the host at create (engine_host.h).
+struct EnvTables {
+    int32_t padMap[NUM_PADS];    // RLGymCPP pad index (CommonValues::BOOST_LOCATIONS) -> arena pad
+    uint32_t ground[3], air[3], jump[3], boost[3];  // DefaultAction masks as 90-bit sets
+    float kickRot[2][NUM_KICKOFF_SPAWNS][9];         // kickoff bases (rows), blue / orange
+    float kickX[NUM_KICKOFF_SPAWNS], kickY[NUM_KICKOFF_SPAWNS];
+};
+
+struct RewardParams {
+    float w[4];               // GoalReward, TouchBallReward, VelocityBallToGoal, VelocityPlayerToBall
+    float concede, teamSpirit, oppScale;
+    int32_t zeroSum;          // bit k: reward k wrapped in ZeroSumReward
+    int32_t episodeMaxTicks;  // truncation after this many ticks since the reset (0 = off)
+    float noTouchTimeout;     // NoTouchCondition seconds (0 = off)
+    float goalBaseY, ballRadius;
+};
+
+struct EnvView {
+    uint32_t* ball;
+    uint32_t* car;
+    uint32_t* pad;
+    uint32_t* arena;
+    int N;
+    const int32_t* teamSize;
+    const int32_t* carOffset;
+    CtlRec* controls;
+    float* obs;
+    int stride;
+    uint8_t* masks;
+    float* rewards;
+    uint8_t* terminals;
+};
+
+// word indices inside the records
+#define RSB_W(T, f) ((int)(offsetof(T, f) / 4))
+constexpr int BW_POS = RSB_W(BallP, pos), BW_ROT = RSB_W(BallP, rot), BW_LIN = RSB_W(BallP, lin), BW_ANG = RSB_W(BallP, ang);
+constexpr int CW_POS = RSB_W(CarP, pos), CW_ROT = RSB_W(CarP, rot), CW_LIN = RSB_W(CarP, lin), CW_ANG = RSB_W(CarP, ang);
+constexpr int CW_BOOST = RSB_W(CarP, boost), CW_AIRSJ = RSB_W(CarP, airTimeSinceJump);
+constexpr int CW_WCN = RSB_W(CarP, worldContactNormal), CW_FLAGS = RSB_W(CarP, flags);
+constexpr int CW_HIT = RSB_W(CarP, ballHitTick), CW_HITX = RSB_W(CarP, ballHitExtraTick), CW_ROTMAT = RSB_W(CarP, rotMat);
+constexpr int CW_STATE0 = RSB_W(CarP, boost), CW_STATE1 = RSB_W(CarP, steerAngle);  // CarState words
+constexpr int AW_TICK = RSB_W(ArenaP, tick), AW_EPISODE = RSB_W(ArenaP, episodeTicks), AW_STATUS = RSB_W(ArenaP, status);
+constexpr int AW_GOALTEAM = RSB_W(ArenaP, goalTeam), AW_TOUCHED = RSB_W(ArenaP, touchedMask);
+constexpr int AW_NOTOUCH = RSB_W(ArenaP, noTouchTimer), AW_SCORED = RSB_W(ArenaP, scored);
+#undef RSB_W
+
+RSB_D uint32_t ballW(const EnvView& E, int a, int w) { return E.ball[(size_t)w * E.N + a]; }
+RSB_D uint32_t carW(const EnvView& E, int a, int s, int w) { return E.car[((size_t)w * MAX_CARS + s) * E.N + a]; }
+RSB_D float ballF(const EnvView& E, int a, int w) { return __uint_as_float(ballW(E, a, w)); }
+RSB_D float carF(const EnvView& E, int a, int s, int w) { return __uint_as_float(carW(E, a, s, w)); }
+
+// RocketSim Vec::Dot with its fourth (zero) component: ((x*x' + y*y') + z*z') + 0*0
+RSB_D float vdot4(float ax, float ay, float az, float bx, float by, float bz) {
+    return ((ax * bx + ay * by) + az * bz) + 0.f;
+}
+
+// ------------------------------------------------------------------ observations
+
+// Per-arena inputs staged in shared memory, one column per arena of the warp.
+constexpr int OBS_ARENAS = 32;
+constexpr int OI_BALL = 0;                                   // pos, vel, ang (uu)
+constexpr int OI_CAR = 9;                                    // per car, OI_CAR_N words
+constexpr int OI_CAR_N = 20;                                 // pos vel ang fwd right up boost flags
+constexpr int OI_PREV = OI_CAR + MAX_CARS * OI_CAR_N;        // per car, 8 action values
+constexpr int OI_PAD = OI_PREV + MAX_CARS * 8;               // 2 frames x 34 pad values
+constexpr int OI_MASK = OI_PAD + 2 * NUM_PADS;               // per car, 3 mask words
+constexpr int OI_TEAM = OI_MASK + MAX_CARS * 3;              // team size
+constexpr int OI_WORDS = OI_TEAM + 1;
+// flag bits of the staged car
+constexpr uint32_t OF_GROUND = 1, OF_FLIPJUMP = 2, OF_DEMOED = 4, OF_JUMPED = 8, OF_ORANGE = 16;
+
+struct ObsShared {
+    float in[OI_WORDS][OBS_ARENAS];
+    uint16_t rowOf[OBS_ARENAS * MAX_CARS];   // local row -> arena (low byte) | slot << 8
+};
+
+RSB_D float obsCarValue(const ObsShared& S, int la, int q, bool inv, int j) {
+    const int o = OI_CAR + q * OI_CAR_N;
+    auto g = [&](int k) { return S.in[o + k][la]; };
+    // InvertPhys: x and y of every vector negated
+    auto iv = [&](int k, int comp) { float v = g(k + comp); return (inv && comp < 2) ? -v : v; };
+    if (j < 3) return iv(0, j) * OBS_POS;
+    if (j < 6) return iv(9, j - 3);
+    if (j < 9) return iv(15, j - 6);
+    if (j < 12) return iv(3, j - 9) * OBS_VEL;
+    if (j < 15) return iv(6, j - 12) * OBS_ANG;
+    if (j < 24) {
+        // rotMat.Dot(v) = (v.forward, v.right, v.up)
+        int r = (j - 15) % 3, kind = (j - 15) / 3;
+        int bk = 9 + 3 * r;
+        float bx = iv(bk, 0), by = iv(bk, 1), bz = iv(bk, 2);
+        float vx, vy, vz, coef;
+        if (kind == 0) {
+            vx = iv(6, 0); vy = iv(6, 1); vz = iv(6, 2);
+            coef = OBS_ANG;
+        } else {
+            int bo = kind == 1 ? 0 : 3;  // ball pos / vel in the staged ball block
+            float cx = S.in[OI_BALL + bo + 0][la], cy = S.in[OI_BALL + bo + 1][la], cz = S.in[OI_BALL + bo + 2][la];
+            if (inv) { cx = -cx; cy = -cy; }
+            vx = cx - iv(bo, 0); vy = cy - iv(bo, 1); vz = cz - iv(bo, 2);
+            coef = kind == 1 ? OBS_POS : OBS_VEL;
+        }
+        return vdot4(vx, vy, vz, bx, by, bz) * coef;
+    }
+    if (j == 24) return g(18) / 100.f;
+    uint32_t f = __float_as_uint(g(19));
+    if (j == 25) return (f & OF_GROUND) ? 1.f : 0.f;
+    if (j == 26) return (f & OF_FLIPJUMP) ? 1.f : 0.f;
+    if (j == 27) return (f & OF_DEMOED) ? 1.f : 0.f;
+    return (f & OF_JUMPED) ? 1.f : 0.f;
+}
+
+// Element `col` of the observation row of slot p in local arena la.
+RSB_D float obsValue(const ObsShared& S, int la, int p, int col) {
+    const int T = (int)S.in[OI_TEAM][la];
+    const int M = 2 * T;
+    const bool orange = p >= T;
+    if (col < 9) {
+        float v = S.in[OI_BALL + col][la] * (col < 3 ? OBS_POS : (col < 6 ? OBS_VEL : OBS_ANG));
+        return (orange && (col % 3) < 2) ? -v : v;
+    }
+    if (col < 17) return S.in[OI_PREV + p * 8 + (col - 9)][la];
+    if (col < 51) return S.in[OI_PAD + (orange ? NUM_PADS : 0) + (col - 17)][la];
+    int k = (col - 51) / 29, j = (col - 51) - 29 * ((col - 51) / 29);
+    if (k >= M) return 0.f;  // rows of smaller arenas in a ragged batch are zero-padded
+    int q;
+    const int ownFirst = orange ? T : 0, oppFirst = orange ? 0 : T;
+    if (k == 0) {
+        q = p;
+    } else if (k < T) {
+        // teammates, descending slot order, skipping the player
+        int idx = k - 1;
+        q = ownFirst + T - 1 - idx;
+        if (q <= p) q--;
+    } else {
+        q = oppFirst + T - 1 - (k - T);
+    }
+    return obsCarValue(S, la, q, orange, j);
+}
+
+__global__ void __launch_bounds__(32) obsKernel(EnvView E, EnvTables Tb) {
+    __shared__ ObsShared S;
+    const int lane = threadIdx.x;
+    const int a0 = blockIdx.x * OBS_ARENAS;
+    if (a0 >= E.N) return;
+    const int aEnd = min(a0 + OBS_ARENAS, E.N);
+    const int a = a0 + lane;
+    const int row0 = E.carOffset[a0];
+    if (a < aEnd) {
+        const int T = E.teamSize[a], M = 2 * T;
+        S.in[OI_TEAM][lane] = (float)T;
+        for (int k = 0; k < 3; k++) {
+            S.in[OI_BALL + k][lane] = ballF(E, a, BW_POS + k) * kBtToUu;
+            S.in[OI_BALL + 3 + k][lane] = ballF(E, a, BW_LIN + k) * kBtToUu;
+            S.in[OI_BALL + 6 + k][lane] = ballF(E, a, BW_ANG + k);
+        }
+        const int base = E.carOffset[a];
+        for (int s = 0; s < M; s++) {
+            const int o = OI_CAR + s * OI_CAR_N;
+            for (int k = 0; k < 3; k++) {
+                S.in[o + k][lane] = carF(E, a, s, CW_POS + k) * kBtToUu;
+                S.in[o + 3 + k][lane] = carF(E, a, s, CW_LIN + k) * kBtToUu;
+                S.in[o + 6 + k][lane] = carF(E, a, s, CW_ANG + k);
+                // CarState::rotMat columns: forward, right, up (basis rows stored)
+                S.in[o + 9 + k][lane] = carF(E, a, s, CW_ROTMAT + 3 * k + 0);
+                S.in[o + 12 + k][lane] = carF(E, a, s, CW_ROTMAT + 3 * k + 1);
+                S.in[o + 15 + k][lane] = carF(E, a, s, CW_ROTMAT + 3 * k + 2);
+            }
+            const float boost = carF(E, a, s, CW_BOOST);
+            S.in[o + 18][lane] = boost;
+            const uint32_t cf = carW(E, a, s, CW_FLAGS);
+            const bool ground = cf & CF_ON_GROUND;
+            // CarState::HasFlipOrJump (Car.cpp:285-289)
+            const bool flipJump = ground || (!(cf & CF_HAS_FLIPPED) && !(cf & CF_HAS_DOUBLE_JUMPED) &&
+                                             carF(E, a, s, CW_AIRSJ) < DOUBLEJUMP_MAX_DELAY);
+            uint32_t of = (ground ? OF_GROUND : 0u) | (flipJump ? OF_FLIPJUMP : 0u) |
+                          ((cf & CF_DEMOED) ? OF_DEMOED : 0u) | ((cf & CF_HAS_JUMPED) ? OF_JUMPED : 0u) |
+                          ((cf & CF_TEAM_ORANGE) ? OF_ORANGE : 0u);
+            S.in[o + 19][lane] = __uint_as_float(of);
+            // DefaultAction::GetActionMask
+            const bool turtled = (cf & CF_WORLD_CONTACT) && carF(E, a, s, CW_WCN + 2) > 0.9f;
+            for (int w = 0; w < 3; w++) {
+                uint32_t m = ground ? Tb.ground[w] : Tb.air[w];
+                if (boost == 0.f) m &= ~Tb.boost[w];
+                if (flipJump || turtled) m |= Tb.jump[w];
+                S.in[OI_MASK + s * 3 + w][lane] = __uint_as_float(m);
+            }
+            // the step's action (EnvSet passes the parsed Action as prevAction)
+            const CtlRec c = E.controls[base + s];
+            for (int k = 0; k < 5; k++) S.in[OI_PREV + s * 8 + k][lane] = c.v[k];
+            S.in[OI_PREV + s * 8 + 5][lane] = c.jump ? 1.f : 0.f;
+            S.in[OI_PREV + s * 8 + 6][lane] = c.boost ? 1.f : 0.f;
+            S.in[OI_PREV + s * 8 + 7][lane] = c.handbrake ? 1.f : 0.f;
+            S.rowOf[base - row0 + s] = (uint16_t)(lane | (s << 8));
+        }
+        // boost pads in RLGymCPP order; GameState::GetBoostPadTimers returns the mirrored
+        // timers for the blue frame and the direct ones for the orange frame
+        // (GameState.h:56-62), and AdvancedObs pairs them with the frame's pads
+        float cool[NUM_PADS];
+        uint32_t act = 0, act2 = 0;
+        for (int p = 0; p < NUM_PADS; p++) {
+            cool[p] = __uint_as_float(E.pad[((size_t)0 * NUM_PADS + p) * E.N + a]);
+            uint32_t bits = E.pad[((size_t)1 * NUM_PADS + p) * E.N + a];
+            if (bits & 1u) {
+                if (p < 32) act |= 1u << p;
+                else act2 |= 1u << (p - 32);
+            }
+        }
+        auto active = [&](int p) { return p < 32 ? ((act >> p) & 1u) : ((act2 >> (p - 32)) & 1u); };
+        for (int i = 0; i < NUM_PADS; i++) {
+            const int d = Tb.padMap[i], m = Tb.padMap[NUM_PADS - 1 - i];
+            S.in[OI_PAD + i][lane] = active(d) ? 1.f : 1.f / (1.f + cool[m]);
+            S.in[OI_PAD + NUM_PADS + i][lane] = active(m) ? 1.f : 1.f / (1.f + cool[d]);
+        }
+    }
+    __syncwarp();
+    const int rows = E.carOffset[aEnd] - row0;
+    const int stride = E.stride;
+    float* out = E.obs + (size_t)row0 * stride;
+    const int n = rows * stride;
+    for (int e = lane; e < n; e += 32) {
+        const int r = e / stride, col = e - r * stride;
+        const uint16_t ro = S.rowOf[r];
+        out[e] = obsValue(S, ro & 0xff, ro >> 8, col);
+    }
+    // masks: rows * 90 bytes, 4-byte aligned (every arena has an even number of cars)
+    uint32_t* mout = reinterpret_cast<uint32_t*>(E.masks + (size_t)row0 * RSB_NUM_ACTIONS);
+    const int nw = rows * RSB_NUM_ACTIONS / 4;
+    for (int w = lane; w < nw; w += 32) {
+        uint32_t word = 0;
+        for (int t = 0; t < 4; t++) {
+            const int e = 4 * w + t, r = e / RSB_NUM_ACTIONS, i = e - r * RSB_NUM_ACTIONS;
+            const uint16_t ro = S.rowOf[r];
+            const uint32_t m = __float_as_uint(S.in[OI_MASK + (ro >> 8) * 3 + (i >> 5)][ro & 0xff]);
+            word |= ((m >> (i & 31)) & 1u) << (8 * t);
+        }
+        mout[w] = word;
+    }
+}
+
+// ------------------------------------------------------------------ rewards and terminals
+
+__global__ void rewardKernel(EnvView E, RewardParams R, int stepTicks) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= E.N) return;
+    const int T = E.teamSize[a], M = 2 * T, base = E.carOffset[a];
+    const float bx = ballF(E, a, BW_POS + 0) * kBtToUu, by = ballF(E, a, BW_POS + 1) * kBtToUu,
+                bz = ballF(E, a, BW_POS + 2) * kBtToUu;
+    const float bvx = ballF(E, a, BW_LIN + 0) * kBtToUu, bvy = ballF(E, a, BW_LIN + 1) * kBtToUu,
+                bvz = ballF(E, a, BW_LIN + 2) * kBtToUu;
+    const uint64_t tick = (uint64_t)E.arena[(size_t)AW_TICK * E.N + a] |
+                          ((uint64_t)E.arena[(size_t)(AW_TICK + 1) * E.N + a] << 32);
+    // GameState::UpdateFromArena: tickSkip = ticks since the last update
+    const uint64_t skip = min((uint64_t)(stepTicks > 0 ? stepTicks : 0), tick);
+    bool touched[MAX_CARS];
+    bool anyTouch = false;
+    for (int s = 0; s < M; s++) {
+        const uint32_t cf = carW(E, a, s, CW_FLAGS);
+        const uint64_t hit = (uint64_t)carW(E, a, s, CW_HIT) | ((uint64_t)carW(E, a, s, CW_HIT + 1) << 32);
+        touched[s] = (cf & CF_BALL_HIT_VALID) && hit >= tick - skip;
+        anyTouch |= touched[s];
+    }
+    // Arena::IsBallScored (Arena.cpp:949-957)
+    const bool goal = fabsf(by) > (R.goalBaseY + R.ballRadius);
+
+    // terminals (EnvSet.cpp:184-205): a normal terminal beats a truncation
+    uint8_t type = 0;
+    if (R.noTouchTimeout > 0.f) {
+        float t = __uint_as_float(E.arena[(size_t)AW_NOTOUCH * E.N + a]);
+        if (anyTouch) {
+            t = 0.f;
+        } else {
+            t += (float)(int)skip * (1 / 120.f);
+            if (t >= R.noTouchTimeout) type = 2;
+        }
+        E.arena[(size_t)AW_NOTOUCH * E.N + a] = __float_as_uint(t);
+    }
+    if (R.episodeMaxTicks > 0 && (int32_t)E.arena[(size_t)AW_EPISODE * E.N + a] >= R.episodeMaxTicks && type == 0)
+        type = 2;
+    if (goal) type = 1;
+    E.terminals[a] = type;
+
+    float all[MAX_CARS];
+    for (int s = 0; s < M; s++) all[s] = 0.f;
+    for (int k = 0; k < 4; k++) {
+        if (R.w[k] == 0.f) continue;
+        float out[MAX_CARS];
+        for (int s = 0; s < M; s++) {
+            const bool orange = s >= T;
+            float r;
+            if (k == 0) {
+                // GoalReward: RS_TEAM_FROM_Y(ball y) is the team whose half holds the ball
+                r = goal ? ((orange != (by >= 0.f)) ? 1.f : R.concede) : 0.f;
+            } else if (k == 1) {
+                r = touched[s] ? 1.f : 0.f;
+            } else if (k == 2) {
+                // VelocityBallToGoalReward: toward CommonValues::ORANGE_GOAL_BACK for blue
+                const float tx = 0.f, ty = orange ? -CV_BACK_NET_Y : CV_BACK_NET_Y, tz = CV_GOAL_HEIGHT / 2;
+                float dx = tx - bx, dy = ty - by, dz = tz - bz;
+                float l2 = vdot4(dx, dy, dz, dx, dy, dz);
+                float l = l2 > 0.f ? sqrtf(l2) : 0.f;
+                if (l > kEpsilon * kEpsilon) { dx = dx / l; dy = dy / l; dz = dz / l; }
+                else { dx = dy = dz = 0.f; }
+                r = vdot4(dx, dy, dz, bvx / CV_BALL_MAX_SPEED, bvy / CV_BALL_MAX_SPEED, bvz / CV_BALL_MAX_SPEED);
+            } else {
+                // VelocityPlayerToBallReward
+                const float px = carF(E, a, s, CW_POS + 0) * kBtToUu, py = carF(E, a, s, CW_POS + 1) * kBtToUu,
+                            pz = carF(E, a, s, CW_POS + 2) * kBtToUu;
+                const float vx = carF(E, a, s, CW_LIN + 0) * kBtToUu, vy = carF(E, a, s, CW_LIN + 1) * kBtToUu,
+                            vz = carF(E, a, s, CW_LIN + 2) * kBtToUu;
+                float dx = bx - px, dy = by - py, dz = bz - pz;
+                float l2 = vdot4(dx, dy, dz, dx, dy, dz);
+                float l = l2 > 0.f ? sqrtf(l2) : 0.f;
+                if (l > kEpsilon * kEpsilon) { dx = dx / l; dy = dy / l; dz = dz / l; }
+                else { dx = dy = dz = 0.f; }
+                r = vdot4(dx, dy, dz, vx / CV_CAR_MAX_SPEED, vy / CV_CAR_MAX_SPEED, vz / CV_CAR_MAX_SPEED);
+            }
+            out[s] = r;
+        }
+        if (R.zeroSum & (1 << k)) {
+            // ZeroSumReward::GetAllRewards over the players in Arena::_cars order
+            int cnt[2] = {0, 0};
+            float avg[2] = {0.f, 0.f};
+            for (int s = M - 1; s >= 0; s--) {
+                const int t = s >= T;
+                cnt[t]++;
+                avg[t] += out[s];
+            }
+            for (int t = 0; t < 2; t++) avg[t] /= (float)(cnt[t] > 1 ? cnt[t] : 1);
+            for (int s = 0; s < M; s++) {
+                const int t = s >= T;
+                out[s] = out[s] * (1 - R.teamSpirit) + (avg[t] * R.teamSpirit) - (avg[1 - t] * R.oppScale);
+            }
+        }
+        for (int s = 0; s < M; s++) all[s] += out[s] * R.w[k];
+    }
+    for (int s = 0; s < M; s++) E.rewards[base + s] = all[s];
+}
+
+// ------------------------------------------------------------------ resets
+
+// Counter-based draws for the resets: splitmix64 of (seed, arena, counter).
+struct ResetRng {
+    uint64_t key;
+    uint32_t ctr;
+    RSB_D uint32_t next() {
+        uint64_t z = key + 0x9E3779B97F4A7C15ull * (uint64_t)(++ctr);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return (uint32_t)((z ^ (z >> 31)) >> 32);
+    }
+    // RocketSim Math::RandFloat: min + u * (max - min), u in [0, 1]
+    RSB_D float uni(float lo, float hi) { return lo + ((float)(next() >> 8) * (1.f / 16777216.f)) * (hi - lo); }
+};
+
+RSB_D V3 randNormVec(ResetRng& g) {
+    V3 v{g.uni(-1, 1), g.uni(-1, 1), g.uni(-1, 1)};
+    return rsNormalized(v);
+}
+
+RSB_D void putCarW(const EnvView& E, int a, int s, int w, uint32_t v) {
+    E.car[((size_t)w * MAX_CARS + s) * E.N + a] = v;
+}
+RSB_D void putCarF(const EnvView& E, int a, int s, int w, float v) { putCarW(E, a, s, w, __float_as_uint(v)); }
+
+// Car::SetState of a default CarState with the given placement (Car.cpp:23-36,
+// Car.h:15-100): the transform, the velocities and every CarState field are replaced;
+// the broadphase registration and the vehicle's wheel values are kept.
+RSB_D void resetCar(const EnvView& E, int a, int s, V3 posUu, const M3& rot, V3 velUu, V3 ang, float boost) {
+    const uint32_t team = carW(E, a, s, CW_FLAGS) & CF_TEAM_ORANGE;
+    const V3 p = posUu * kUuToBt, v = velUu * kUuToBt;
+    const float pv[3] = {p.x, p.y, p.z}, vv[3] = {v.x, v.y, v.z}, av[3] = {ang.x, ang.y, ang.z};
+    for (int k = 0; k < 3; k++) {
+        putCarF(E, a, s, CW_POS + k, pv[k]);
+        putCarF(E, a, s, CW_LIN + k, vv[k]);
+        putCarF(E, a, s, CW_ANG + k, av[k]);
+        putCarF(E, a, s, CW_ROT + 3 * k + 0, rot.r[k].x);
+        putCarF(E, a, s, CW_ROT + 3 * k + 1, rot.r[k].y);
+        putCarF(E, a, s, CW_ROT + 3 * k + 2, rot.r[k].z);
+    }
+    // CarState words (boost .. lastCtlBits): defaults, then the placement
+    for (int w = CW_STATE0; w < CW_STATE1; w++) putCarW(E, a, s, w, 0u);
+    putCarF(E, a, s, CW_BOOST, boost);
+    putCarW(E, a, s, CW_FLAGS, CF_ON_GROUND | team);
+    for (int k = 0; k < 2; k++) {
+        putCarW(E, a, s, CW_HIT + k, 0xffffffffu);
+        putCarW(E, a, s, CW_HITX + k, 0xffffffffu);
+    }
+    for (int k = 0; k < 3; k++) {
+        putCarF(E, a, s, CW_ROTMAT + 3 * k + 0, rot.r[k].x);
+        putCarF(E, a, s, CW_ROTMAT + 3 * k + 1, rot.r[k].y);
+        putCarF(E, a, s, CW_ROTMAT + 3 * k + 2, rot.r[k].z);
+    }
+}
+
+RSB_D M3 rowsToM3(const float* r) { return m3(r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8]); }
+
+// Angle(yaw, pitch, roll).ToRotMat() = btMatrix3x3::setEulerYPR(yaw, -pitch, -roll)
+// (MathTypes.cpp:73-78)
+RSB_D M3 angleRot(float yaw, float pitch, float roll) { return m3fromEulerZYX(-roll, -pitch, yaw); }
+
+// Arena i of the list `idx` (every arena when idx is null; with `onlyDone`, only the
+// arenas whose terminal flag is set).
+__global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, uint64_t seed, int mode,
+                            bool onlyDone) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int a = idx ? idx[i] : i;
+    if (onlyDone && E.terminals[a] == 0) return;
+    const int T = E.teamSize[a], M = 2 * T, base = E.carOffset[a];
+    ResetRng g{seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(a + 1)), 0};
+    constexpr float PI = 3.14159265358979323846f;
+
+    // kickoff layout (always applied first, as RandomState does): a shuffled spawn per
+    // kickoff rank, rank i of each team taking the i-th car in Arena::_cars order
+    int order[NUM_KICKOFF_SPAWNS] = {0, 1, 2, 3, 4};
+    for (int k = NUM_KICKOFF_SPAWNS - 1; k > 0; k--) {
+        int j = (int)(g.next() % (uint32_t)(k + 1));
+        int t = order[k]; order[k] = order[j]; order[j] = t;
+    }
+    for (int r = 0; r < T; r++) {
+        const int sp = order[r];
+        for (int team = 0; team < 2; team++) {
+            const int s = team * T + (T - 1 - r);
+            V3 pos{Tb.kickX[sp], Tb.kickY[sp], CAR_SPAWN_REST_Z};
+            if (team) pos = pos * V3{-1.f, -1.f, 1.f};
+            resetCar(E, a, s, pos, rowsToM3(Tb.kickRot[team][sp]), v3zero(), v3zero(), BOOST_SPAWN_AMOUNT);
+        }
+    }
+    V3 ballPos{0.f, 0.f, BALL_REST_Z}, ballVel = v3zero(), ballAng = v3zero();
+
+    if (mode == RSB_RESET_RANDOM_STATE) {
+        // RandomState(randBallSpeed, randCarSpeed, carsOnGround = false)
+        const float X = 3500.f, Y = 4000.f, Z = 1820.f;
+        ballPos = V3{g.uni(-X, X), g.uni(-Y, Y), g.uni(CV_BALL_RADIUS, Z)};
+        ballVel = randNormVec(g) * g.uni(0.f, 4000.f);
+        ballAng = V3{g.uni(-4.f, 4.f), g.uni(-4.f, 4.f), g.uni(-4.f, 4.f)};
+        for (int s = M - 1; s >= 0; s--) {
+            V3 pos{g.uni(-X, X), g.uni(-Y, Y), g.uni(150.f, Z)};
+            V3 vel = randNormVec(g) * g.uni(0.f, CV_CAR_MAX_SPEED);
+            V3 ang = randNormVec(g) * 5.5f;
+            float yaw = g.uni(-PI, PI), pitch = g.uni(-PI / 2, PI / 2), roll = g.uni(-PI, PI);
+            const bool onGround = g.uni(0.f, 1.f) > 0.5f;
+            if (onGround) {
+                pos.z = CAR_SPAWN_REST_Z;
+                pitch = roll = 0.f;
+                vel.z = 0.f;
+                ang = v3zero();
+            }
+            resetCar(E, a, s, pos, angleRot(yaw, pitch, roll), vel, ang, g.uni(0.f, 100.f));
+        }
+    } else if (mode == RSB_RESET_HIGH_CONTACT) {
+        // cars within 300 uu of the ball or of another car, 1500-2300 uu/s toward it,
+        // half airborne; some start on a side wall or under the ceiling
+        ballPos = V3{g.uni(-3000.f, 3000.f), g.uni(-3600.f, 3600.f), g.uni(CV_BALL_RADIUS, 1200.f)};
+        ballVel = randNormVec(g) * g.uni(0.f, 1500.f);
+        V3 prev = ballPos;
+        bool prevFree = false;  // the previous car is a free start (a valid anchor)
+        for (int s = M - 1; s >= 0; s--) {
+            const V3 anchor = (prevFree && g.uni(0.f, 1.f) >= 0.5f) ? prev : ballPos;
+            const float kind = g.uni(0.f, 1.f);
+            V3 pos;
+            float pitch = 0.f, roll = 0.f;
+            bool air = g.uni(0.f, 1.f) < 0.5f;
+            const bool free = kind >= 0.15f;
+            if (kind < 0.1f) {
+                // side wall start, wheels on the wall
+                const float side = g.uni(0.f, 1.f) < 0.5f ? -1.f : 1.f;
+                pos = V3{side * 4000.f, g.uni(-3500.f, 3500.f), g.uni(300.f, 1500.f)};
+                roll = side * (PI / 2);
+                air = true;
+            } else if (!free) {
+                // under the ceiling, upside down
+                pos = V3{g.uni(-3000.f, 3000.f), g.uni(-3800.f, 3800.f), 1950.f};
+                roll = PI;
+                air = true;
+            } else {
+                // within 150-300 uu (horizontally) of the anchor
+                const float r = g.uni(150.f, 300.f), t = g.uni(-PI, PI);
+                pos = V3{anchor.x + r * cosf(t), anchor.y + r * sinf(t), 0.f};
+                pos.z = air ? fminf(fmaxf(anchor.z + g.uni(-300.f, 300.f), 150.f), 1900.f) : CAR_SPAWN_REST_Z;
+            }
+            V3 to = anchor - pos;
+            if (!air) to.z = 0.f;
+            V3 dir = rsNormalized(to);
+            if (dir == v3zero()) dir = V3{1.f, 0.f, 0.f};
+            const V3 vel = dir * g.uni(1500.f, 2300.f);
+            const float yaw = atan2f(dir.y, dir.x);
+            if (air && free) pitch = g.uni(-PI / 4, PI / 4);
+            resetCar(E, a, s, pos, angleRot(yaw, pitch, roll), vel, v3zero(), g.uni(0.f, 100.f));
+            prev = pos;
+            prevFree = free;
+        }
+    }
+
+    // Ball::SetState (Ball.cpp:35-49) of a BallState with that placement
+    uint32_t* ball = E.ball;
+    const V3 bp = ballPos * kUuToBt, bv = ballVel * kUuToBt;
+    const float bpv[3] = {bp.x, bp.y, bp.z}, bvv[3] = {bv.x, bv.y, bv.z}, bav[3] = {ballAng.x, ballAng.y, ballAng.z};
+    for (int k = 0; k < 3; k++) {
+        ball[(size_t)(BW_POS + k) * E.N + a] = __float_as_uint(bpv[k]);
+        ball[(size_t)(BW_LIN + k) * E.N + a] = __float_as_uint(bvv[k]);
+        ball[(size_t)(BW_ANG + k) * E.N + a] = __float_as_uint(bav[k]);
+        for (int c = 0; c < 3; c++) ball[(size_t)(BW_ROT + 3 * k + c) * E.N + a] = __float_as_uint(k == c ? 1.f : 0.f);
+    }
+    // BoostPad::SetState(BoostPadState())
+    uint32_t* pad = E.pad;
+    for (int p = 0; p < NUM_PADS; p++) {
+        pad[((size_t)0 * NUM_PADS + p) * E.N + a] = __float_as_uint(0.f);
+        pad[((size_t)1 * NUM_PADS + p) * E.N + a] = 1u;
+    }
+    E.arena[(size_t)AW_EPISODE * E.N + a] = 0;
+    E.arena[(size_t)AW_STATUS * E.N + a] = 0;
+    E.arena[(size_t)AW_GOALTEAM * E.N + a] = (uint32_t)-1;
+    E.arena[(size_t)AW_TOUCHED * E.N + a] = 0;
+    E.arena[(size_t)AW_NOTOUCH * E.N + a] = 0;
+    // every reset places the ball inside the field (|y| <= 4000 uu), short of a goal line
+    E.arena[(size_t)AW_SCORED * E.N + a] = 0;
+    // the new state's players carry default (zero) actions
+    for (int s = 0; s < M; s++) E.controls[base + s] = CtlRec{};
+}
+
+}  // namespace rsb

@@ -19,6 +19,7 @@
 #include "rsb.h"
 #include "arena_build.h"
 #include "engine_host.h"
+#include "env_kernels.cuh"
 
 using namespace rsb;
 
@@ -93,6 +94,16 @@ struct rsb_handle {
     rsb_controls* dLut = nullptr;
     int lutCount = 0;
     int32_t* dActions = nullptr;
+    // env layer
+    int obsStride = 0;
+    float* dObs = nullptr;
+    uint8_t* dMasks = nullptr;
+    float* dRewards = nullptr;
+    uint8_t* dTerminals = nullptr;
+    int32_t* dResetIdx = nullptr;
+    EnvTables tables{};
+    bool hasRewards = false;
+    RewardParams rewardParams{};
     std::string err;
     rsb_stats stats{};
 };
@@ -155,6 +166,24 @@ static EngineView devView(rsb_handle* h) {
     return D;
 }
 
+static EnvView envView(rsb_handle* h) {
+    EnvView E;
+    E.ball = h->dBall;
+    E.car = h->dCar;
+    E.pad = h->dPad;
+    E.arena = h->dArena;
+    E.N = h->N;
+    E.teamSize = h->dTeamSize;
+    E.carOffset = h->dCarOffset;
+    E.controls = reinterpret_cast<CtlRec*>(h->dControls);
+    E.obs = h->dObs;
+    E.stride = h->obsStride;
+    E.masks = h->dMasks;
+    E.rewards = h->dRewards;
+    E.terminals = h->dTerminals;
+    return E;
+}
+
 static cudaStream_t pick(rsb_handle* h, void* s) { return s ? (cudaStream_t)s : h->stream; }
 
 // ------------------------------------------------------------------ C ABI
@@ -215,6 +244,22 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     if (cfg->mutators) h->mut = *cfg->mutators;
     else defaultMutators(&h->mut);
     computeParams(h->mut, h->P);
+    h->obsStride = RSB_OBS_BASE + RSB_OBS_PER_CAR * h->maxCars;
+    if (!buildEnvTables(h->tables)) return fail(nullptr, RSB_ERR_STATE, "boost pad tables do not match");
+    if (cfg->rewards) {
+        const rsb_reward_config& r = *cfg->rewards;
+        h->hasRewards = true;
+        RewardParams& R = h->rewardParams;
+        R.w[0] = r.w_goal; R.w[1] = r.w_touch; R.w[2] = r.w_vel_ball_to_goal; R.w[3] = r.w_vel_player_to_ball;
+        R.concede = r.goal_concede_scale;
+        R.teamSpirit = r.team_spirit;
+        R.oppScale = r.opponent_scale;
+        R.zeroSum = r.zero_sum;
+        R.episodeMaxTicks = r.episode_max_ticks;
+        R.noTouchTimeout = r.no_touch_timeout_s;
+        R.goalBaseY = h->mut.goal_base_threshold_y;
+        R.ballRadius = h->mut.ball_radius;
+    }
 
     // static arena data (host build shared across handles, device copy per device)
     std::string folder(cfg->meshes_path);
@@ -273,7 +318,11 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
         !dalloc(h->dBall, (size_t)W_BALL * N * 4) || !dalloc(h->dCar, (size_t)W_CAR * MAX_CARS * N * 4) ||
         !dalloc(h->dPad, (size_t)W_PAD * NUM_PADS * N * 4) || !dalloc(h->dArena, (size_t)W_ARENA * N * 4) ||
         !dalloc(h->dControls, std::max<size_t>(1, h->numCars) * sizeof(rsb_controls)) ||
-        !dalloc(h->dActions, std::max<size_t>(1, h->numCars) * 4))
+        !dalloc(h->dActions, std::max<size_t>(1, h->numCars) * 4) ||
+        !dalloc(h->dObs, (size_t)h->numCars * h->obsStride * 4) ||
+        !dalloc(h->dMasks, (size_t)h->numCars * RSB_NUM_ACTIONS) ||
+        !dalloc(h->dRewards, (size_t)h->numCars * 4) || !dalloc(h->dTerminals, N) ||
+        !dalloc(h->dResetIdx, N * 4))
         return fail(nullptr, RSB_ERR_NOMEM, "device allocation failed");
     cudaMemcpy(h->dTeamSize, h->teamSize.data(), N * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(h->dCarOffset, h->carOffset.data(), (N + 1) * 4, cudaMemcpyHostToDevice);
@@ -296,6 +345,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->dTeamSize); cudaFree(h->dCarOffset); cudaFree(h->dBall); cudaFree(h->dCar);
     cudaFree(h->dPad); cudaFree(h->dArena); cudaFree(h->dControls); cudaFree(h->dLut); cudaFree(h->dActions);
+    cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return RSB_OK;
@@ -534,28 +584,95 @@ rsb_status rsb_last_error(const rsb_handle* h, char* buf, size_t n) {
 rsb_status rsb_device_ptr(rsb_handle* h, int32_t which, void** out) {
     if (!h || !out) return RSB_ERR_INVALID;
     switch (which) {
+        case RSB_BUF_OBS: *out = h->dObs; return RSB_OK;
+        case RSB_BUF_MASKS: *out = h->dMasks; return RSB_OK;
+        case RSB_BUF_REWARDS: *out = h->dRewards; return RSB_OK;
+        case RSB_BUF_TERMINALS: *out = h->dTerminals; return RSB_OK;
         case RSB_BUF_CONTROLS: *out = h->dControls; return RSB_OK;
         case RSB_BUF_ACTIONS: *out = h->dActions; return RSB_OK;
-        default: return fail(h, RSB_ERR_UNSUPPORTED, "buffer not built into this library yet");
+        default: return fail(h, RSB_ERR_INVALID, "unknown buffer");
     }
 }
 
-rsb_status rsb_reset_all(rsb_handle* h, uint64_t, int32_t) {
-    return fail(h, RSB_ERR_UNSUPPORTED, "resets are not built into this library yet");
+rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* idx, int32_t n, uint64_t seed, int32_t mode) {
+    if (!h || n < 0 || (n > 0 && !idx) || n > h->N) return fail(h, RSB_ERR_INVALID, "bad reset arena list");
+    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_HIGH_CONTACT) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
+    for (int i = 0; i < n; i++)
+        if (idx[i] < 0 || idx[i] >= h->N) return fail(h, RSB_ERR_INVALID, "arena index out of range");
+    if (n == 0) return RSB_OK;
+    RSB_CUDA(cudaSetDevice(h->device));
+    RSB_CUDA(cudaMemcpyAsync(h->dResetIdx, idx, 4 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+    resetKernel<<<(n + 127) / 128, 128, 0, h->stream>>>(envView(h), h->tables, h->dResetIdx, n, seed, mode, false);
+    RSB_CUDA(cudaGetLastError());
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
 }
-rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t*, int32_t, uint64_t, int32_t) {
-    return fail(h, RSB_ERR_UNSUPPORTED, "resets are not built into this library yet");
+
+rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode) {
+    if (!h) return RSB_ERR_INVALID;
+    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_HIGH_CONTACT) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
+    RSB_CUDA(cudaSetDevice(h->device));
+    resetKernel<<<(h->N + 127) / 128, 128, 0, h->stream>>>(envView(h), h->tables, nullptr, h->N, seed, mode, false);
+    RSB_CUDA(cudaGetLastError());
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
 }
+
+rsb_status rsb_reset_done(rsb_handle* h, uint64_t seed, int32_t mode, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_HIGH_CONTACT) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
+    RSB_CUDA(cudaSetDevice(h->device));
+    resetKernel<<<(h->N + 127) / 128, 128, 0, pick(h, stream)>>>(envView(h), h->tables, nullptr, h->N, seed, mode, true);
+    RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
 rsb_status rsb_default_action_lut(rsb_controls* out, int32_t cap) {
     if (!out || cap < RSB_NUM_ACTIONS) return RSB_ERR_INVALID;
     return defaultActionLut(out, cap) == RSB_NUM_ACTIONS ? RSB_OK : RSB_ERR_STATE;
 }
-rsb_status rsb_snapshot(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
-rsb_status rsb_build_obs(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
-rsb_status rsb_build_rewards_terminals(rsb_handle* h, int32_t, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
-rsb_status rsb_copy_obs(rsb_handle* h, float*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
-rsb_status rsb_copy_masks(rsb_handle* h, uint8_t*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
-rsb_status rsb_copy_rewards(rsb_handle* h, float*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
-rsb_status rsb_copy_terminals(rsb_handle* h, uint8_t*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not built yet"); }
+
+// The four stub rewards read no state from before the step (CommonRewards.h:33-98), so
+// there is nothing to copy; the call stays for the reference's call sequence.
+rsb_status rsb_snapshot(rsb_handle* h, void*) { return h ? RSB_OK : RSB_ERR_INVALID; }
+
+rsb_status rsb_build_obs(rsb_handle* h, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    RSB_CUDA(cudaSetDevice(h->device));
+    obsKernel<<<(h->N + OBS_ARENAS - 1) / OBS_ARENAS, 32, 0, pick(h, stream)>>>(envView(h), h->tables);
+    RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+rsb_status rsb_build_rewards_terminals(rsb_handle* h, int32_t step_ticks, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    if (!h->hasRewards) return fail(h, RSB_ERR_STATE, "no reward configuration at create");
+    RSB_CUDA(cudaSetDevice(h->device));
+    rewardKernel<<<(h->N + 127) / 128, 128, 0, pick(h, stream)>>>(envView(h), h->rewardParams, step_ticks);
+    RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+static rsb_status copyOut(rsb_handle* h, void* out, const void* dev, size_t count, size_t expect, size_t elem,
+                          const char* what) {
+    if (!h || !out) return RSB_ERR_INVALID;
+    if (count != expect) return fail(h, RSB_ERR_INVALID, std::string(what) + ": count must equal the buffer size");
+    RSB_CUDA(cudaSetDevice(h->device));
+    RSB_CUDA(cudaMemcpyAsync(out, dev, count * elem, cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
+}
+rsb_status rsb_copy_obs(rsb_handle* h, float* out, size_t n) {
+    return copyOut(h, out, h ? h->dObs : nullptr, n, h ? (size_t)h->numCars * h->obsStride : 0, 4, "obs");
+}
+rsb_status rsb_copy_masks(rsb_handle* h, uint8_t* out, size_t n) {
+    return copyOut(h, out, h ? h->dMasks : nullptr, n, h ? (size_t)h->numCars * RSB_NUM_ACTIONS : 0, 1, "masks");
+}
+rsb_status rsb_copy_rewards(rsb_handle* h, float* out, size_t n) {
+    return copyOut(h, out, h ? h->dRewards : nullptr, n, h ? (size_t)h->numCars : 0, 4, "rewards");
+}
+rsb_status rsb_copy_terminals(rsb_handle* h, uint8_t* out, size_t n) {
+    return copyOut(h, out, h ? h->dTerminals : nullptr, n, h ? (size_t)h->N : 0, 1, "terminals");
+}
 
 }  // extern "C"

@@ -30,6 +30,8 @@ RSB_OBS_PER_CAR = 29
 RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS = range(6)
 RSB_CULL_EXACT, RSB_CULL_LEARNED = 0, 1
 RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT = 0, 1, 2
+RSB_ARENA_NONFINITE, RSB_ARENA_ROW_OVERFLOW, RSB_ARENA_BVH_OVERFLOW, RSB_ARENA_CULL_MISS, RSB_ARENA_EPA_OVERFLOW = (
+    1, 2, 4, 8, 16)
 
 _STATUS = {
     -1: "RSB_ERR_INVALID", -2: "RSB_ERR_CUDA", -3: "RSB_ERR_NOMEM", -4: "RSB_ERR_MESH",
@@ -71,10 +73,10 @@ class CarState(C.Structure):
         ("has_flipped", C.c_uint8), ("is_flipping", C.c_uint8), ("is_jumping", C.c_uint8),
         ("is_supersonic", C.c_uint8), ("is_auto_flipping", C.c_uint8), ("is_demoed", C.c_uint8),
         ("world_contact", C.c_uint8), ("ball_hit_valid", C.c_uint8), ("team", C.c_uint8),
-        ("wheels_with_contact", C.c_uint8 * 4),
+        ("wheels_with_contact", C.c_uint8 * 4), ("pad1_", C.c_uint32),
         ("ball_hit_tick", C.c_uint64), ("ball_hit_extra_tick", C.c_uint64),
         ("ball_hit_rel_pos", Vec3), ("ball_hit_ball_pos", Vec3), ("ball_hit_extra_vel", Vec3),
-        ("last_controls", Controls), ("id", C.c_uint32), ("pad_", C.c_uint32),
+        ("last_controls", Controls), ("id", C.c_uint32), ("pad_", C.c_uint32), ("pad2_", C.c_uint32),
     ]
 
 
@@ -150,6 +152,7 @@ _SIGS = {
     "rsb_set_actions_device": [_P, _P, C.c_int32, _P],
     "rsb_set_controls": [_P, _P, C.c_int32],
     "rsb_step": [_P, C.c_int32, _P],
+    "rsb_reset_done": [_P, C.c_uint64, C.c_int32, _P],
     "rsb_snapshot": [_P, _P],
     "rsb_build_obs": [_P, _P],
     "rsb_build_rewards_terminals": [_P, C.c_int32, _P],
@@ -200,6 +203,17 @@ def default_mutators(lib: C.CDLL) -> Mutators:
     m = Mutators()
     lib.rsb_default_mutators(C.byref(m))
     return m
+
+
+def default_rewards(lib: C.CDLL, **overrides) -> RewardConfig:
+    """rsb_default_rewards, then the given fields replaced (e.g. zero_sum=0b1111)."""
+    r = RewardConfig()
+    st = lib.rsb_default_rewards(C.byref(r))
+    if st != 0:
+        raise RsbError(st, "rsb_default_rewards failed")
+    for k, v in overrides.items():
+        setattr(r, k, v)
+    return r
 
 
 def default_action_lut(lib: C.CDLL) -> np.ndarray:
@@ -317,6 +331,10 @@ class Batch:
     def reset_arenas(self, idx, seed: int, mode: int = RSB_RESET_KICKOFF):
         a = np.ascontiguousarray(idx, np.int32)
         self._check(self.lib.rsb_reset_arenas(self._h, _ptr(a), len(a), seed, mode))
+
+    def reset_done(self, seed: int, mode: int = RSB_RESET_KICKOFF, stream: int | None = None):
+        """Resets the arenas whose terminal flag is set (device-side, stream-ordered)."""
+        self._check(self.lib.rsb_reset_done(self._h, seed, mode, C.c_void_p(stream or 0)))
 
     def set_action_lut(self, lut: np.ndarray):
         lut = np.ascontiguousarray(lut, CONTROLS_DTYPE)

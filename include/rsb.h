@@ -79,7 +79,8 @@ enum {
     RSB_BUF_OBS = 0,        /* float [num_cars][obs_stride] */
     RSB_BUF_MASKS = 1,      /* uint8 [num_cars][90] */
     RSB_BUF_REWARDS = 2,    /* float [num_cars] */
-    RSB_BUF_TERMINALS = 3,  /* uint8 [num_arenas]: 0 none, 1 goal, 2 timeout */
+    RSB_BUF_TERMINALS = 3,  /* uint8 [num_arenas]: RLGymCPP TerminalType: 0 none, 1 normal
+                               (goal), 2 truncated (no touch / episode tick limit) */
     RSB_BUF_CONTROLS = 4,   /* rsb_controls [num_cars] */
     RSB_BUF_ACTIONS = 5     /* int32 [num_cars] */
 };
@@ -93,8 +94,11 @@ enum {
 /* Reset modes for rsb_reset_arenas. */
 enum {
     RSB_RESET_KICKOFF = 0,      /* RocketSim Arena::ResetToRandomKickoff layout */
-    RSB_RESET_RANDOM_STATE = 1, /* uniform random cars/ball inside the field */
-    RSB_RESET_HIGH_CONTACT = 2  /* cars near the ball / each other, fast, half airborne */
+    RSB_RESET_RANDOM_STATE = 1, /* RLGymCPP RandomState(true, true, false): uniform random
+                                   cars/ball inside the field, half the cars on the ground */
+    RSB_RESET_HIGH_CONTACT = 2  /* cars within 300 uu of the ball or each other, 1500-2300
+                                   uu/s toward it, half airborne, some on walls / ceiling
+                                   (no CPU counterpart in the reference) */
 };
 
 typedef struct rsb_vec3 { float x, y, z; } rsb_vec3;
@@ -128,12 +132,13 @@ typedef struct rsb_car_state {
     uint8_t is_flipping, is_jumping, is_supersonic, is_auto_flipping;
     uint8_t is_demoed, world_contact, ball_hit_valid, team; /* team: 0 blue, 1 orange */
     uint8_t wheels_with_contact[4];
+    uint32_t pad1_;                  /* explicit padding (always 0) */
     uint64_t ball_hit_tick;          /* ~0 when never */
     uint64_t ball_hit_extra_tick;    /* tick of the last extra car-ball impulse, ~0 when never */
     rsb_vec3 ball_hit_rel_pos, ball_hit_ball_pos, ball_hit_extra_vel;
     rsb_controls last_controls;
     uint32_t id;
-    uint32_t pad_;
+    uint32_t pad_, pad2_;            /* explicit padding (always 0) */
 } rsb_car_state;
 
 /* RocketSim BallState (Sim/Ball/Ball.h:15-45), soccar fields. */
@@ -194,8 +199,10 @@ typedef struct rsb_reward_config {
     float goal_concede_scale;     /* GoalReward's concedeScale (default -1) */
     float team_spirit;            /* ZeroSumReward teamSpirit */
     float opponent_scale;         /* ZeroSumReward opponentScale */
-    int32_t zero_sum;             /* 1: wrap rewards in ZeroSumReward */
-    int32_t episode_max_ticks;    /* timeout terminal (0 = off) */
+    int32_t zero_sum;             /* bit k wraps reward k (goal, touch, ball-to-goal velocity,
+                                     player-to-ball velocity) in ZeroSumReward */
+    int32_t episode_max_ticks;    /* truncation after this many ticks since the arena's
+                                     reset (0 = off) */
     float no_touch_timeout_s;     /* NoTouchCondition (0 = off) */
 } rsb_reward_config;
 
@@ -245,6 +252,12 @@ rsb_status rsb_layout(const rsb_handle* h, int32_t* num_arenas, int32_t* num_car
 rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride);
 
 rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode);
+/* Resets every arena whose terminal flag (from the last rsb_build_rewards_terminals) is
+ * set, on the device and stream-ordered, with no host round trip; the flags themselves
+ * are left as they are.  Pass a different seed on every call.  No counterpart in the
+ * reference: CudaEnvSet::ResetTerminalArenasGpu (CudaEnvSet.cpp:182-200) reads the
+ * flags back to the host and calls RocketSimCudaBatch::ResetArena per arena. */
+rsb_status rsb_reset_done(rsb_handle* h, uint64_t seed, int32_t mode, void* stream);
 rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* arena_idx, int32_t n,
                             uint64_t seed, int32_t mode);
 

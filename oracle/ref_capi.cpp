@@ -14,9 +14,23 @@
 //   - Ball::GetState / SetState         Ball.cpp:27-49
 //   - BoostPad::GetState / SetState     BoostPad.h:45-46
 //   - Arena::IsBallScored               Arena.cpp:949-957
+//   - the collector's env step          RLGymCPP EnvSet.cpp:117-260, 392-424 (GameState,
+//                                       AdvancedObs, DefaultAction masks, the four stub
+//                                       rewards, ZeroSumReward, terminal conditions,
+//                                       kickoff / RandomState resets), run with
+//                                       RLGymCPP's own classes
 #include "rsb.h"
 
 #include "RocketSim.h"
+#include "RLGymCPP/ActionParsers/DefaultAction.h"
+#include "RLGymCPP/Gamestates/GameState.h"
+#include "RLGymCPP/ObsBuilders/AdvancedObs.h"
+#include "RLGymCPP/RewardCore/CommonRewards.h"
+#include "RLGymCPP/RewardCore/RuntimeRewardRegistry.h"
+#include "RLGymCPP/RewardCore/ZeroSumReward.h"
+#include "RLGymCPP/StateSetters/RandomState.h"
+#include "RLGymCPP/TerminalConditions/GoalScoreCondition.h"
+#include "RLGymCPP/TerminalConditions/NoTouchCondition.h"
 
 #include <atomic>
 #include <cstring>
@@ -26,6 +40,23 @@
 #include <vector>
 
 using namespace RocketSim;
+
+// Env state of one arena: what EnvSet keeps per arena for the collector's path
+// (EnvSet.cpp:117-260): the reward list (each optionally wrapped in ZeroSumReward) and
+// the terminal conditions, plus the actions of the last step for the observations.
+struct OracleEnv {
+    std::vector<std::pair<RLGC::Reward*, float>> rewards;
+    std::vector<RLGC::TerminalCondition*> terminals;
+};
+
+// Truncation after a fixed number of ticks since the last reset (the learner's episode cap).
+struct EpisodeTickLimit : RLGC::TerminalCondition {
+    const int32_t* ticks;
+    int32_t limit;
+    EpisodeTickLimit(const int32_t* t, int32_t l) : ticks(t), limit(l) {}
+    bool IsTerminal(const RLGC::GameState&) override { return *ticks >= limit; }
+    bool IsTruncation() override { return true; }
+};
 
 struct rsb_handle {
     std::vector<Arena*> arenas;
@@ -39,9 +70,17 @@ struct rsb_handle {
     int32_t threads = 1;
     std::string err;
     rsb_stats stats{};
+    // env layer
+    bool hasRewards = false;
+    rsb_reward_config rewardCfg{};
+    std::vector<OracleEnv> env;
+    std::vector<float> obs, rewardsOut;
+    std::vector<uint8_t> masks, terminalsOut;
 };
 
 static std::string g_createError;
+static void buildEnv(rsb_handle* h);
+static void freeEnv(rsb_handle* h);
 static std::mutex g_initMutex;
 static bool g_inited = false;
 
@@ -158,6 +197,30 @@ static CarState toCarState(const rsb_car_state& o) {
     return s;
 }
 
+// Runs fn(a) for every arena on the handle's host threads (EnvSet runs its per-arena
+// work on a thread pool in the same way, EnvSet.cpp:113-260).
+template <class Fn>
+static void forArenas(rsb_handle* h, Fn fn) {
+    int n = (int)h->arenas.size();
+    int t = std::min(h->threads, n);
+    if (t <= 1) {
+        for (int a = 0; a < n; a++) fn(a);
+        return;
+    }
+    std::vector<std::thread> pool;
+    std::atomic<int> next{0};
+    const int chunk = 4;
+    for (int i = 0; i < t; i++)
+        pool.emplace_back([&] {
+            for (;;) {
+                int a0 = next.fetch_add(chunk);
+                if (a0 >= n) break;
+                for (int a = a0; a < std::min(n, a0 + chunk); a++) fn(a);
+            }
+        });
+    for (auto& th : pool) th.join();
+}
+
 extern "C" {
 
 rsb_status rsb_default_mutators(rsb_mutators* m) {
@@ -241,12 +304,18 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     }
     h->controls.assign(h->numCars, rsb_controls{});
     h->episodeTicks.assign(cfg->num_arenas, 0);
+    if (cfg->rewards) {
+        h->hasRewards = true;
+        h->rewardCfg = *cfg->rewards;
+        buildEnv(h);
+    }
     *out = h;
     return RSB_OK;
 }
 
 rsb_status rsb_destroy(rsb_handle* h) {
     if (!h) return RSB_ERR_INVALID;
+    freeEnv(h);
     for (Arena* a : h->arenas) delete a;
     delete h;
     return RSB_OK;
@@ -303,25 +372,8 @@ static void stepRange(rsb_handle* h, int a0, int a1, int ticks) {
 
 rsb_status rsb_step(rsb_handle* h, int32_t ticks, void*) {
     if (!h || ticks < 0) return fail(h, RSB_ERR_INVALID, "bad tick count");
-    int n = (int)h->arenas.size();
-    int t = std::min(h->threads, n);
-    if (t <= 1) {
-        stepRange(h, 0, n, ticks);
-    } else {
-        std::vector<std::thread> pool;
-        std::atomic<int> next{0};
-        const int chunk = 4;
-        for (int i = 0; i < t; i++)
-            pool.emplace_back([&] {
-                for (;;) {
-                    int a0 = next.fetch_add(chunk);
-                    if (a0 >= n) break;
-                    stepRange(h, a0, std::min(n, a0 + chunk), ticks);
-                }
-            });
-        for (auto& th : pool) th.join();
-    }
-    h->stats.ticks_simulated += (uint64_t)n * ticks;
+    forArenas(h, [&](int a) { stepRange(h, a, a + 1, ticks); });
+    h->stats.ticks_simulated += (uint64_t)h->arenas.size() * ticks;
     return RSB_OK;
 }
 
@@ -464,19 +516,200 @@ rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride) {
     return RSB_OK;
 }
 
-// Env-layer entry points (resets, observations, rewards) are added with the env layer.
-rsb_status rsb_default_rewards(rsb_reward_config*) { return RSB_ERR_UNSUPPORTED; }
-rsb_status rsb_reset_all(rsb_handle* h, uint64_t, int32_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t*, int32_t, uint64_t, int32_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_default_action_lut(rsb_controls*, int32_t) { return RSB_ERR_UNSUPPORTED; }
+rsb_status rsb_default_action_lut(rsb_controls* lut, int32_t count) {
+    // RLGymCPP's DefaultAction table (DefaultAction.cpp:3-91), converted the way
+    // EnvSet hands actions to the cars: (CarControls)action (Action.h:32-45)
+    static RLGC::DefaultAction parser;
+    if (!lut || count < (int32_t)parser.actions.size()) return RSB_ERR_INVALID;
+    for (size_t i = 0; i < parser.actions.size(); i++) lut[i] = fromControls((CarControls)parser.actions[i]);
+    return (int32_t)parser.actions.size() == RSB_NUM_ACTIONS ? RSB_OK : RSB_ERR_STATE;
+}
+
 rsb_status rsb_set_actions_device(rsb_handle* h, const int32_t*, int32_t, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "no device on the CPU oracle"); }
-rsb_status rsb_snapshot(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_build_obs(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_build_rewards_terminals(rsb_handle* h, int32_t, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_copy_obs(rsb_handle* h, float*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_copy_masks(rsb_handle* h, uint8_t*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_copy_rewards(rsb_handle* h, float*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
-rsb_status rsb_copy_terminals(rsb_handle* h, uint8_t*, size_t) { return fail(h, RSB_ERR_UNSUPPORTED, "not available"); }
 rsb_status rsb_device_ptr(rsb_handle* h, int32_t, void**) { return fail(h, RSB_ERR_UNSUPPORTED, "no device on the CPU oracle"); }
 
+rsb_status rsb_default_rewards(rsb_reward_config* r) {
+    if (!r) return RSB_ERR_INVALID;
+    *r = rsb_reward_config{};
+    r->w_goal = r->w_touch = r->w_vel_ball_to_goal = r->w_vel_player_to_ball = 1.f;
+    r->goal_concede_scale = -1.f;
+    r->team_spirit = 0.f;
+    r->opponent_scale = 1.f;
+    r->zero_sum = 0;
+    r->episode_max_ticks = 1800;
+    r->no_touch_timeout_s = 0.f;
+    return RSB_OK;
+}
+
 }  // extern "C"
+
+// The env-layer entry points below keep the C linkage of their declarations in rsb.h.
+
+static void buildEnv(rsb_handle* h) {
+    const rsb_reward_config& rc = h->rewardCfg;
+    h->env.resize(h->arenas.size());
+    for (size_t a = 0; a < h->arenas.size(); a++) {
+        OracleEnv& e = h->env[a];
+        auto add = [&](RLGC::Reward* r, float w, int bit) {
+            if (w == 0.f) { delete r; return; }
+            if (rc.zero_sum & (1 << bit)) r = new RLGC::ZeroSumReward(r, rc.team_spirit, rc.opponent_scale);
+            e.rewards.emplace_back(r, w);
+        };
+        add(new RLGC::GoalReward(rc.goal_concede_scale), rc.w_goal, 0);
+        add(new RLGC::TouchBallReward(), rc.w_touch, 1);
+        add(new RLGC::VelocityBallToGoalReward(), rc.w_vel_ball_to_goal, 2);
+        add(new RLGC::VelocityPlayerToBallReward(), rc.w_vel_player_to_ball, 3);
+        if (rc.no_touch_timeout_s > 0.f) e.terminals.push_back(new RLGC::NoTouchCondition(rc.no_touch_timeout_s));
+        e.terminals.push_back(new RLGC::GoalScoreCondition());
+        if (rc.episode_max_ticks > 0) e.terminals.push_back(new EpisodeTickLimit(&h->episodeTicks[a], rc.episode_max_ticks));
+    }
+}
+
+static void freeEnv(rsb_handle* h) {
+    for (auto& e : h->env) {
+        for (auto& r : e.rewards) delete r.first;
+        for (auto* t : e.terminals) delete t;
+    }
+    h->env.clear();
+}
+
+// Slot (creation index) of every entry of Arena::_cars, in iteration order.
+static std::vector<int> carsOrder(rsb_handle* h, size_t a) {
+    std::vector<int> order;
+    for (Car* c : h->arenas[a]->GetCars())
+        for (size_t s = 0; s < h->cars[a].size(); s++)
+            if (h->cars[a][s] == c) order.push_back((int)s);
+    return order;
+}
+
+// GameState::UpdateFromArena with the actions of the last step in the arena's car
+// order; lastTickCount set so that the state's tickSkip is step_ticks.
+static void gameStateOf(rsb_handle* h, size_t a, int stepTicks, RLGC::GameState& gs, std::vector<int>& order) {
+    order = carsOrder(h, a);
+    std::vector<RLGC::Action> actions(order.size());
+    for (size_t i = 0; i < order.size(); i++)
+        actions[i] = RLGC::Action(toControls(h->controls[h->carOffset[a] + order[i]]));
+    uint64_t tc = h->arenas[a]->tickCount;
+    gs = RLGC::GameState();
+    gs.lastTickCount = tc - std::min<uint64_t>((uint64_t)std::max(stepTicks, 0), tc);
+    gs.UpdateFromArena(h->arenas[a], actions, nullptr);
+}
+
+rsb_status rsb_snapshot(rsb_handle* h, void*) {
+    // the four stub rewards read no previous state (CommonRewards.h:33-98)
+    return h ? RSB_OK : RSB_ERR_INVALID;
+}
+
+rsb_status rsb_build_obs(rsb_handle* h, void*) {
+    if (!h) return RSB_ERR_INVALID;
+    static RLGC::DefaultAction parser;
+    RLGC::AdvancedObs builder;
+    int32_t stride = 0;
+    rsb_obs_stride(h, &stride);
+    h->obs.assign((size_t)h->numCars * stride, 0.f);
+    h->masks.assign((size_t)h->numCars * RSB_NUM_ACTIONS, 0);
+    forArenas(h, [&](int a) {
+        RLGC::GameState gs;
+        std::vector<int> order;
+        gameStateOf(h, a, 0, gs, order);
+        for (size_t i = 0; i < order.size(); i++) {
+            size_t row = h->carOffset[a] + order[i];
+            RLGC::FList o = builder.BuildObs(gs.players[i], gs);
+            std::copy(o.begin(), o.end(), h->obs.begin() + row * stride);
+            std::vector<uint8_t> m = parser.GetActionMask(gs.players[i], gs);
+            std::copy(m.begin(), m.end(), h->masks.begin() + row * RSB_NUM_ACTIONS);
+        }
+    });
+    return RSB_OK;
+}
+
+rsb_status rsb_build_rewards_terminals(rsb_handle* h, int32_t step_ticks, void*) {
+    if (!h) return RSB_ERR_INVALID;
+    if (!h->hasRewards) return fail(h, RSB_ERR_STATE, "no reward configuration at create");
+    h->rewardsOut.assign(h->numCars, 0.f);
+    h->terminalsOut.assign(h->arenas.size(), 0);
+    forArenas(h, [&](int a) {
+        RLGC::GameState gs;
+        std::vector<int> order;
+        gameStateOf(h, a, step_ticks, gs, order);
+        // EnvSet.cpp:184-205: every condition is evaluated; normal beats truncation
+        uint8_t type = RLGC::TerminalType::NOT_TERMINAL;
+        for (auto* cond : h->env[a].terminals) {
+            if (cond->IsTerminal(gs)) {
+                uint8_t cur = cond->IsTruncation() ? RLGC::TerminalType::TRUNCATED : RLGC::TerminalType::NORMAL;
+                if (type == RLGC::TerminalType::NOT_TERMINAL || cur == RLGC::TerminalType::NORMAL) type = cur;
+            }
+        }
+        h->terminalsOut[a] = type;
+        // EnvSet.cpp:207-254
+        std::vector<float> all(order.size(), 0.f);
+        for (auto& wr : h->env[a].rewards) wr.first->PreStep(gs);
+        for (auto& wr : h->env[a].rewards) {
+            std::vector<float> out = wr.first->GetAllRewards(gs, type);
+            float scale = RLGC::RuntimeRewardScale(wr.first->GetName(), wr.second);
+            for (size_t i = 0; i < order.size(); i++) all[i] += out[i] * scale;
+        }
+        for (size_t i = 0; i < order.size(); i++) h->rewardsOut[h->carOffset[a] + order[i]] = all[i];
+    });
+    return RSB_OK;
+}
+
+template <class T>
+static rsb_status copyOut(rsb_handle* h, const std::vector<T>& src, T* out, size_t count, const char* what) {
+    if (!h || !out) return RSB_ERR_INVALID;
+    if (count != src.size()) return fail(h, RSB_ERR_INVALID, std::string(what) + ": count does not match (build it first)");
+    std::memcpy(out, src.data(), count * sizeof(T));
+    return RSB_OK;
+}
+rsb_status rsb_copy_obs(rsb_handle* h, float* out, size_t n) { return copyOut(h, h->obs, out, n, "obs"); }
+rsb_status rsb_copy_masks(rsb_handle* h, uint8_t* out, size_t n) { return copyOut(h, h->masks, out, n, "masks"); }
+rsb_status rsb_copy_rewards(rsb_handle* h, float* out, size_t n) { return copyOut(h, h->rewardsOut, out, n, "rewards"); }
+rsb_status rsb_copy_terminals(rsb_handle* h, uint8_t* out, size_t n) { return copyOut(h, h->terminalsOut, out, n, "terminals"); }
+
+// EnvSet::ResetArena (EnvSet.cpp:392-424): state setter, then the terminal conditions
+// and rewards are reset; the new state's players carry default (zero) actions.
+static void resetOne(rsb_handle* h, int a, uint64_t seed, int32_t mode) {
+    Arena* arena = h->arenas[a];
+    if (mode == RSB_RESET_KICKOFF) {
+        arena->ResetToRandomKickoff((int)(uint32_t)(seed ^ (seed >> 32) ^ (0x9E3779B9u * (uint32_t)(a + 1))) & 0x7fffffff);
+    } else {
+        RLGC::RandomState(true, true, false).ResetArena(arena);
+    }
+    for (size_t c = 0; c < h->cars[a].size(); c++) h->controls[h->carOffset[a] + c] = rsb_controls{};
+    h->episodeTicks[a] = 0;
+    if (!h->env.empty()) {
+        RLGC::GameState gs(arena);
+        for (auto* t : h->env[a].terminals) t->Reset(gs);
+        for (auto& r : h->env[a].rewards) r.first->Reset(gs);
+    }
+}
+
+rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* idx, int32_t n, uint64_t seed, int32_t mode) {
+    if (!h || (n > 0 && !idx)) return RSB_ERR_INVALID;
+    if (mode != RSB_RESET_KICKOFF && mode != RSB_RESET_RANDOM_STATE)
+        return fail(h, RSB_ERR_UNSUPPORTED, "the CPU oracle has kickoff and random-state resets only");
+    for (int i = 0; i < n; i++)
+        if (idx[i] < 0 || idx[i] >= (int32_t)h->arenas.size()) return fail(h, RSB_ERR_INVALID, "arena index out of range");
+    for (int i = 0; i < n; i++) resetOne(h, idx[i], seed, mode);
+    return RSB_OK;
+}
+
+rsb_status rsb_reset_done(rsb_handle* h, uint64_t seed, int32_t mode, void*) {
+    if (!h) return RSB_ERR_INVALID;
+    if (mode != RSB_RESET_KICKOFF && mode != RSB_RESET_RANDOM_STATE)
+        return fail(h, RSB_ERR_UNSUPPORTED, "the CPU oracle has kickoff and random-state resets only");
+    if (h->terminalsOut.size() != h->arenas.size()) return RSB_OK;
+    forArenas(h, [&](int a) {
+        if (h->terminalsOut[a]) resetOne(h, a, seed, mode);
+    });
+    return RSB_OK;
+}
+
+rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode) {
+    if (!h) return RSB_ERR_INVALID;
+    std::vector<int32_t> idx(h->arenas.size());
+    for (size_t a = 0; a < idx.size(); a++) idx[a] = (int32_t)a;
+    return rsb_reset_arenas(h, idx.data(), (int32_t)idx.size(), seed, mode);
+}
+
+

@@ -138,6 +138,7 @@ def run_ours(args, rank, world, dist):
                       meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank, rewards=rewards)
     batch.reset_all(0x5EED0001 + rank, rsb.RSB_RESET_RANDOM_STATE)
     batch.set_action_lut(rsb.default_action_lut(batch.lib))
+
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -166,6 +167,8 @@ def run_ours(args, rank, world, dist):
         for _ in range(args.warmup):
             one_step()
     torch.cuda.synchronize()
+    # pick the step kernel's launch configuration on a copy of the warmed-up state
+    tune = batch.autotune(wl.tick_skip) if not args.no_autotune else []
     if dist is not None:
         dist.barrier()
     times, step_times = [], []
@@ -233,6 +236,7 @@ def run_ours(args, rank, world, dist):
                 "d2h_bytes_per_step": int(statistics.mean(d2h))},
         # per env step: action expansion, step, obs + masks, rewards + terminals, reset
         "gpu_launches": args.steps * 5,
+        "autotune": tune,
         "clocks": clocks.summary(),
     }
     return res
@@ -291,16 +295,20 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--arenas", type=int, default=8192)
-    ap.add_argument("--team-size", type=int, default=2)
+    ap.add_argument("--arenas", type=int, default=65536)
+    ap.add_argument("--team-size", type=int, default=3)
     ap.add_argument("--tick-skip", type=int, default=8)
-    ap.add_argument("--workload-name",
-                    default="soccar 2v2 x 8192 arenas, tickSkip 8: random discrete actions -> 8 ticks -> "
-                            "AdvancedObs + masks -> 4 stub rewards + terminals -> random-state resets")
+    ap.add_argument("--workload-name", default=None)
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload_name is None:
+        t = args.team_size
+        args.workload_name = (f"soccar {t}v{t} x {args.arenas} arenas, tickSkip {args.tick_skip}: random discrete "
+                              f"actions -> {args.tick_skip} ticks -> AdvancedObs + masks -> 4 stub rewards + "
+                              "terminals -> random-state resets")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -101,6 +101,9 @@ struct rsb_handle {
     float* dRewards = nullptr;
     uint8_t* dTerminals = nullptr;
     int32_t* dResetIdx = nullptr;
+    // launch configuration of the step kernel (indices into kStepVariants / kStepBlocks)
+    int stepVariant = 0, stepBlock = 2;
+    uint32_t* dScratch = nullptr;   // the autotuner's copy of the arena records
     EnvTables tables{};
     bool hasRewards = false;
     RewardParams rewardParams{};
@@ -119,7 +122,11 @@ static rsb_status cudaFail(rsb_handle* h, const char* what, cudaError_t e) {
 
 // ------------------------------------------------------------------ kernels
 
-__global__ void __launch_bounds__(128) stepKernel(EngineView D, int ticks) {
+// One thread advances one arena.  MINB is the minimum number of 128-thread blocks per SM
+// the compiler must fit, which caps the registers per thread; the autotuner picks the
+// variant and the block size.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) stepKernel(EngineView D, int ticks) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= D.N) return;
     ArenaSim A;
@@ -127,6 +134,15 @@ __global__ void __launch_bounds__(128) stepKernel(EngineView D, int ticks) {
     A.W.epa = &epa;
     stepArena(D, a, ticks, A);
 }
+
+struct StepVariant {
+    void (*fn)(EngineView, int);
+    int minBlocks;
+};
+static const StepVariant kStepVariants[] = {{stepKernel<1>, 1}, {stepKernel<3>, 3}, {stepKernel<4>, 4}};
+constexpr int kNumStepVariants = sizeof(kStepVariants) / sizeof(kStepVariants[0]);
+static const int kStepBlocks[] = {32, 64, 128};
+constexpr int kNumStepBlocks = sizeof(kStepBlocks) / sizeof(kStepBlocks[0]);
 
 __global__ void expandActionsKernel(const int32_t* idx, const rsb_controls* lut, int lutCount, rsb_controls* out, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -299,11 +315,17 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(nullptr, RSB_ERR_CUDA, "cudaSetDevice failed");
     {
         // the arena kernel keeps one arena's working set in thread-local memory; make the
-        // per-thread stack limit cover its frame (the default limit is 1 KB)
-        cudaFuncAttributes fa{};
-        if (cudaFuncGetAttributes(&fa, stepKernel) != cudaSuccess)
-            return fail(nullptr, RSB_ERR_CUDA, "cudaFuncGetAttributes failed");
-        size_t need = ((fa.localSizeBytes + 4096) + 1023) / 1024 * 1024, cur = 0;
+        // per-thread stack limit cover the largest variant's frame (the default limit is
+        // 1 KB), and give the L1 its largest share (the kernels use no shared memory)
+        size_t need = 0;
+        for (const StepVariant& v : kStepVariants) {
+            cudaFuncAttributes fa{};
+            if (cudaFuncGetAttributes(&fa, v.fn) != cudaSuccess)
+                return fail(nullptr, RSB_ERR_CUDA, "cudaFuncGetAttributes failed");
+            need = std::max(need, ((fa.localSizeBytes + 4096) + 1023) / 1024 * 1024);
+            cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+        }
+        size_t cur = 0;
         cudaDeviceGetLimit(&cur, cudaLimitStackSize);
         if (cur < need && cudaDeviceSetLimit(cudaLimitStackSize, need) != cudaSuccess)
             return fail(nullptr, RSB_ERR_CUDA, "cannot raise the per-thread stack limit for the arena kernel");
@@ -345,6 +367,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->dTeamSize); cudaFree(h->dCarOffset); cudaFree(h->dBall); cudaFree(h->dCar);
     cudaFree(h->dPad); cudaFree(h->dArena); cudaFree(h->dControls); cudaFree(h->dLut); cudaFree(h->dActions);
+    cudaFree(h->dScratch);
     cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -372,10 +395,69 @@ rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
     if (ticks == 0) return RSB_OK;
     RSB_CUDA(cudaSetDevice(h->device));
     EngineView D = devView(h);
-    int block = 128, grid = (h->N + block - 1) / block;
-    stepKernel<<<grid, block, 0, pick(h, stream)>>>(D, ticks);
+    int block = kStepBlocks[h->stepBlock], grid = (h->N + block - 1) / block;
+    kStepVariants[h->stepVariant].fn<<<grid, block, 0, pick(h, stream)>>>(D, ticks);
     RSB_CUDA(cudaGetLastError());
     h->stats.ticks_simulated += (uint64_t)h->N * ticks;
+    return RSB_OK;
+}
+
+rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32_t cap, int32_t* count) {
+    if (!h || ticks <= 0 || cap < 0) return fail(h, RSB_ERR_INVALID, "bad autotune arguments");
+    RSB_CUDA(cudaSetDevice(h->device));
+    const size_t wBall = (size_t)W_BALL * h->N, wCar = (size_t)W_CAR * MAX_CARS * h->N;
+    const size_t wPad = (size_t)W_PAD * NUM_PADS * h->N, wArena = (size_t)W_ARENA * h->N;
+    const size_t words = wBall + wCar + wPad + wArena;
+    if (!h->dScratch && cudaMalloc((void**)&h->dScratch, words * 4) != cudaSuccess)
+        return fail(h, RSB_ERR_NOMEM, "autotune scratch allocation failed");
+    EngineView D = devView(h);
+    D.ball = h->dScratch;
+    D.car = D.ball + wBall;
+    D.pad = D.car + wCar;
+    D.arena = D.pad + wPad;
+    cudaEvent_t e0, e1;
+    RSB_CUDA(cudaEventCreate(&e0));
+    RSB_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int n = 0, bestV = h->stepVariant, bestB = h->stepBlock;
+    rsb_status st = RSB_OK;
+    for (int v = 0; v < kNumStepVariants && st == RSB_OK; v++)
+        for (int b = 0; b < kNumStepBlocks && st == RSB_OK; b++) {
+            float ms = 1e30f;
+            for (int rep = 0; rep < 2; rep++) {
+                // every candidate starts from the same copy of the current state
+                cudaError_t e = cudaMemcpyAsync(D.ball, h->dBall, wBall * 4, cudaMemcpyDeviceToDevice, h->stream);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(D.car, h->dCar, wCar * 4, cudaMemcpyDeviceToDevice, h->stream);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(D.pad, h->dPad, wPad * 4, cudaMemcpyDeviceToDevice, h->stream);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(D.arena, h->dArena, wArena * 4, cudaMemcpyDeviceToDevice, h->stream);
+                const int block = kStepBlocks[b], grid = (h->N + block - 1) / block;
+                if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
+                if (e == cudaSuccess) {
+                    kStepVariants[v].fn<<<grid, block, 0, h->stream>>>(D, ticks);
+                    e = cudaGetLastError();
+                }
+                if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float t = 0.f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+                if (e != cudaSuccess) {
+                    st = cudaFail(h, "autotune candidate", e);
+                    break;
+                }
+                ms = std::min(ms, t);
+            }
+            if (st != RSB_OK) break;
+            if (out && n < cap) out[n] = rsb_tune_entry{kStepVariants[v].minBlocks, kStepBlocks[b], ms};
+            n++;
+            if (ms < best) { best = ms; bestV = v; bestB = b; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != RSB_OK) return st;
+    h->stepVariant = bestV;
+    h->stepBlock = bestB;
+    if (count) *count = n;
     return RSB_OK;
 }
 

@@ -123,6 +123,10 @@ class Config(C.Structure):
                 ("device", C.c_int32), ("threads", C.c_int32)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("min_blocks", C.c_int32), ("block", C.c_int32), ("ms", C.c_float)]
+
+
 class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "ticks_simulated", "narrowphase_queries", "culled_queries", "missed_contacts",
@@ -153,6 +157,7 @@ _SIGS = {
     "rsb_set_controls": [_P, _P, C.c_int32],
     "rsb_step": [_P, C.c_int32, _P],
     "rsb_reset_done": [_P, C.c_uint64, C.c_int32, _P],
+    "rsb_autotune": [_P, C.c_int32, _P, C.c_int32, _P],
     "rsb_snapshot": [_P, _P],
     "rsb_build_obs": [_P, _P],
     "rsb_build_rewards_terminals": [_P, C.c_int32, _P],
@@ -368,6 +373,13 @@ class Batch:
 
     def build_rewards_terminals(self, step_ticks: int, stream: int | None = None):
         self._check(self.lib.rsb_build_rewards_terminals(self._h, step_ticks, C.c_void_p(stream or 0)))
+
+    def autotune(self, ticks: int = 8) -> list[dict]:
+        """rsb_autotune: times the step kernel's launch configurations, keeps the fastest."""
+        out = (TuneEntry * 32)()
+        n = C.c_int32()
+        self._check(self.lib.rsb_autotune(self._h, ticks, out, 32, C.byref(n)))
+        return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms} for e in out[:n.value]]
 
     def sync(self):
         self._check(self.lib.rsb_sync(self._h))

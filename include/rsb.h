@@ -299,6 +299,19 @@ rsb_status rsb_get_pads(rsb_handle* h, rsb_pad_state* out, int32_t n);   /* n = 
 rsb_status rsb_set_pads(rsb_handle* h, const rsb_pad_state* in, int32_t n);
 rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n);
 
+/* One candidate launch configuration of the step kernel and its measured time. */
+typedef struct rsb_tune_entry {
+    int32_t min_blocks;   /* register budget: at least this many 128-thread blocks per SM */
+    int32_t block;        /* threads per block (one arena per thread) */
+    float ms;             /* best of two timed launches of `ticks` ticks */
+} rsb_tune_entry;
+
+/* Times every launch configuration of the step kernel on a device copy of the current
+ * arena state (the handle's own state is not advanced), keeps the fastest for later
+ * rsb_step calls, and reports every candidate in out[0..cap).  Allocates the scratch copy
+ * of the state on its first call.  No counterpart in the reference. */
+rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32_t cap, int32_t* count);
+
 rsb_status rsb_sync(rsb_handle* h);
 rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out);
 /* Copies the last error message (NUL-terminated, truncated to n). Safe with h == NULL

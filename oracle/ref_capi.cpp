@@ -475,6 +475,13 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
 
 rsb_status rsb_sync(rsb_handle* h) { return h ? RSB_OK : RSB_ERR_INVALID; }
 
+// The CPU oracle has a single configuration.
+rsb_status rsb_autotune(rsb_handle* h, int32_t, rsb_tune_entry*, int32_t, int32_t* count) {
+    if (!h) return RSB_ERR_INVALID;
+    if (count) *count = 0;
+    return RSB_OK;
+}
+
 // Oracle-only helpers (not part of include/rsb.h).
 //
 // rsbref_car_order: the order in which the reference visits the cars of arena `a` on

@@ -144,7 +144,7 @@ RSB_HD void arenaTick(ArenaSim& A) {
     ballFinishTick(W, W.ballVelCache);
     if (A.goalTeam < 0 && ballScored(W, W.P->goalBaseY, W.P->ballRadiusUu)) A.goalTeam = W.b[0].xf.o.y > 0 ? 0 : 1;
     A.tickCount++;
-    A.status |= (int32_t)W.status;
+    A.status |= (int32_t)(W.status | W.cullMissed);
     W.status = 0;
 }
 

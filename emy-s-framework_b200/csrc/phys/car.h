@@ -331,6 +331,7 @@ RSB_HD void carSetSpawnState(World& W, int ci, V3 posUu, const M3& rot, float bo
 
 // Car::Respawn for soccar; `pick` selects one of CAR_RESPAWN_LOCATIONS_SOCCAR
 RSB_HD void carRespawn(World& W, int ci, int pick) {
+    W.cull &= ~(1u << (1 + ci));  // the spawn is next to the floor: no culling this launch
     const double kRespawnYaw = 3.14159265358979323846 / 2;
     const float xs[4] = {-2304.f, -2688.f, 2304.f, 2688.f};
     CarSim& c = W.c[ci];

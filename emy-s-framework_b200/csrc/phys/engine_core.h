@@ -24,6 +24,9 @@ struct EngineView {
     uint32_t* arena;
     const CtlRec* controls;
     uint32_t seed;
+    const uint32_t* cull;          // per-arena body bits from the learned culler, or null
+    int32_t cullAudit;             // run culled static tests anyway and count what they find
+    unsigned long long* counters;  // [static tests run, tests culled, culled tests that hit], or null
 };
 
 RSB_HD void initBodyCommon(Body& b) {
@@ -219,7 +222,18 @@ RSB_HD void stepArena(const EngineView& D, int a, int ticks, ArenaSim& A) {
     A.goalTeam = ap.goalTeam;
     A.touchedMask = (uint32_t)ap.touchedMask;
     A.rngKey = mixHash(D.seed, (uint32_t)a, 0x5EEDu);
+    W.cull = D.cull ? D.cull[a] : 0u;
+    W.cullAudit = D.cullAudit;
+    W.nStatic = W.nCulled = W.nMissed = 0;
+    W.cullMissed = 0;
     for (int t = 0; t < ticks; t++) arenaTick(A);
+#if defined(__CUDA_ARCH__)
+    if (D.counters) {
+        atomicAdd(&D.counters[0], (unsigned long long)W.nStatic);
+        atomicAdd(&D.counters[1], (unsigned long long)W.nCulled);
+        if (W.nMissed) atomicAdd(&D.counters[2], (unsigned long long)W.nMissed);
+    }
+#endif
     storeBall(D, a, W.b[0]);
     for (int s = 0; s < A.numCars; s++) storeCar(D, a, s, W.b[1 + s], W.c[s]);
     for (int p = 0; p < NUM_PADS; p++) {

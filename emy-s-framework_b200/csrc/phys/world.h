@@ -38,10 +38,35 @@ struct World {
     uint64_t tick;          // Arena::tickCount at the start of this tick
     V3 ballVelCache;        // Ball::_velocityImpulseCache
     EpaWork* epa;           // EPA scratch (faces and support vertices)
+    // learned culling: bit b set = body b (0 ball, 1 + s car s) is clear of every static
+    // shape for this launch, so its static tests (wheel rays against meshes and planes,
+    // mesh / plane narrowphase) cannot find anything and are skipped; with cullAudit they
+    // run anyway and whatever they find is counted as a miss
+    uint32_t cull;
+    int32_t cullAudit;
+    mutable uint32_t nStatic, nCulled, nMissed;  // static tests run / skipped / skipped but hit
+    mutable uint32_t cullMissed;                 // WS_CULL_MISS once a skipped test would have hit
 };
 
 // world status bits (per-arena status word)
-enum : uint32_t { WS_NONFINITE = 1u, WS_OVERFLOW = 2u, WS_BVH_OVERFLOW = 4u, WS_EPA_OVERFLOW = 16u };
+enum : uint32_t { WS_NONFINITE = 1u, WS_OVERFLOW = 2u, WS_BVH_OVERFLOW = 4u, WS_CULL_MISS = 8u, WS_EPA_OVERFLOW = 16u };
+
+// Bookkeeping of one static test of body b: returns true when the test must be skipped.
+// (nCulled counts the tests the bound clears, also in audit mode where they still run.)
+RSB_HD bool cullSkip(const World& W, int b) {
+    if ((W.cull >> b) & 1u) {
+        W.nCulled++;
+        if (!W.cullAudit) return true;
+    }
+    W.nStatic++;
+    return false;
+}
+RSB_HD void cullCheck(const World& W, int b, bool found) {
+    if (found && ((W.cull >> b) & 1u)) {
+        W.nMissed++;
+        W.cullMissed = WS_CULL_MISS;
+    }
+}
 
 // ------------------------------------------------------------------ objects
 
@@ -317,6 +342,8 @@ RSB_HD void collideBallMesh(World& W, int mesh, Manifold& man) {
     const WorldParams& P = *W.P;
     const Body& ball = W.b[0];
     ObjRef rMesh = objRef(W, mesh), rBall = objRef(W, OBJ_BALL);
+    bool found = false;
+    if (!cullSkip(W, 0)) {
     V3 amn, amx;
     ballAabb(P, ball.xf, amn, amx);  // convexInTriangleSpace == ball transform (mesh at identity)
     M3 invB = inverse(ball.xf.b);
@@ -337,6 +364,7 @@ RSB_HD void collideBallMesh(World& W, int mesh, Manifold& man) {
         V3 point, normal;
         float depth;
         if (sphereTriCollide(v, ball.xf.o, P.ballRadius, man.cbt, point, normal, depth)) {
+            found = true;
             int idx = addContact(man, W.pool, mesh, rMesh, OBJ_BALL, rBall, normal, point, depth);
             if (idx >= 0) {
                 MPoint& cp = man.pt[idx];
@@ -347,6 +375,8 @@ RSB_HD void collideBallMesh(World& W, int mesh, Manifold& man) {
         }
         return true;
     });
+    }
+    cullCheck(W, 0, found);
     if (man.n) refreshContactPoints(man, rBall.xf, rMesh.xf);
 }
 
@@ -358,15 +388,18 @@ RSB_HD void collideBallPlane(World& W, int plane, Manifold& man) {
     float pc = 0.f;
     Xf planeInConvex = xfMul(xfInverse(rBall.xf), rPlane.xf);
     Xf convexInPlane = xfMul(xfInverse(rPlane.xf), rBall.xf);
-    V3 vtx = sphereSupport(planeInConvex.b * (-pn), P.ballMargin);
-    V3 vip = xfPoint(convexInPlane, vtx);
-    float distance = dot(pn, vip) - pc;
-    if (distance < man.cbt + 0.f) {
-        V3 proj = vip - pn * distance;
-        V3 world = xfPoint(rPlane.xf, proj);
-        V3 nb = rPlane.xf.b * pn;
-        int idx = addContact(man, W.pool, plane, rPlane, OBJ_BALL, rBall, nb, world, distance);
-        if (idx >= 0) man.pt[idx].special = 1;
+    if (!cullSkip(W, 0)) {
+        V3 vtx = sphereSupport(planeInConvex.b * (-pn), P.ballMargin);
+        V3 vip = xfPoint(convexInPlane, vtx);
+        float distance = dot(pn, vip) - pc;
+        if (distance < man.cbt + 0.f) {
+            cullCheck(W, 0, true);
+            V3 proj = vip - pn * distance;
+            V3 world = xfPoint(rPlane.xf, proj);
+            V3 nb = rPlane.xf.b * pn;
+            int idx = addContact(man, W.pool, plane, rPlane, OBJ_BALL, rBall, nb, world, distance);
+            if (idx >= 0) man.pt[idx].special = 1;
+        }
     }
     if (man.n) refreshContactPoints(man, rBall.xf, rPlane.xf);
 }
@@ -501,6 +534,8 @@ RSB_HD void collideBoxMesh(World& W, int mesh, int ci, const Xf& childXf, Manifo
     M3 invB = inverse(childXf.b);
     float maxDist2 = sq((C.boxMargin + 0.f) + man.cbt);
     bool responds = carResponds(W, ci);
+    bool found = false;
+    if (!cullSkip(W, 1 + ci)) {
     bvhQueryAabb(*W.S, mesh, amn, amx, [&](int tri) {
         V3 v[3];
         triVerts(*W.S, mesh, tri, v);
@@ -517,6 +552,7 @@ RSB_HD void collideBoxMesh(World& W, int mesh, int ci, const Xf& childXf, Manifo
         GjkOut g = gjkPairDetector(W.epa, box, childXf, triS, xfIdentity(), maxDist2);
         if (g.overflow) W.status |= WS_EPA_OVERFLOW;
         if (g.has) {
+            found = true;
             int idx = addContact(man, W.pool, mesh, rMesh, carObj, rCar, g.normal, g.point, g.dist);
             if (idx >= 0 && responds) {
                 MPoint& cp = man.pt[idx];
@@ -527,6 +563,8 @@ RSB_HD void collideBoxMesh(World& W, int mesh, int ci, const Xf& childXf, Manifo
         }
         return true;
     });
+    }
+    cullCheck(W, 1 + ci, found);
     if (man.n) refreshContactPoints(man, rCar.xf, rMesh.xf);
 }
 
@@ -539,15 +577,18 @@ RSB_HD void collideBoxPlane(World& W, int plane, int ci, const Xf& childXf, Mani
     V3 pn = W.S->planeNormal[plane - MAX_MESHES];
     Xf planeInConvex = xfMul(xfInverse(childXf), rPlane.xf);
     Xf convexInPlane = xfMul(xfInverse(rPlane.xf), childXf);
-    V3 vtx = supportVirtual(box, planeInConvex.b * (-pn));
-    V3 vip = xfPoint(convexInPlane, vtx);
-    float distance = dot(pn, vip) - 0.f;
-    if (distance < man.cbt + 0.f) {
-        V3 proj = vip - pn * distance;
-        V3 world = xfPoint(rPlane.xf, proj);
-        V3 nb = rPlane.xf.b * pn;
-        int idx = addContact(man, W.pool, plane, rPlane, carObj, rCar, nb, world, distance);
-        if (idx >= 0 && carResponds(W, ci)) onCarWorld(W, ci, man.pt[idx]);
+    if (!cullSkip(W, 1 + ci)) {
+        V3 vtx = supportVirtual(box, planeInConvex.b * (-pn));
+        V3 vip = xfPoint(convexInPlane, vtx);
+        float distance = dot(pn, vip) - 0.f;
+        if (distance < man.cbt + 0.f) {
+            cullCheck(W, 1 + ci, true);
+            V3 proj = vip - pn * distance;
+            V3 world = xfPoint(rPlane.xf, proj);
+            V3 nb = rPlane.xf.b * pn;
+            int idx = addContact(man, W.pool, plane, rPlane, carObj, rCar, nb, world, distance);
+            if (idx >= 0 && carResponds(W, ci)) onCarWorld(W, ci, man.pt[idx]);
+        }
     }
     if (man.n) refreshContactPoints(man, rCar.xf, rPlane.xf);
 }
@@ -673,13 +714,24 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
     hit.fraction = 1.f;
     hit.obj = -1;
     hit.normal = v3zero();
+    const int rayBody = ignoreObj - OBJ_BALL;  // the casting car's body
     auto testObj = [&](int o) {
         if (hit.fraction == 0.f) return;
         if (o == ignoreObj) return;
-        if (o < MAX_MESHES) {
-            rayVsMesh(S, o, from, to, hit);
-        } else if (o < NUM_STATICS) {
-            rayVsPlane(S, o, from, to, hit);
+        if (o < NUM_STATICS) {
+            if (cullSkip(W, rayBody)) return;
+            if ((W.cull >> rayBody) & 1u) {
+                // audit: would this static have been hit at all?
+                RayHit probe;
+                probe.fraction = 1.f;
+                probe.obj = -1;
+                probe.normal = v3zero();
+                if (o < MAX_MESHES) rayVsMesh(S, o, from, to, probe);
+                else rayVsPlane(S, o, from, to, probe);
+                cullCheck(W, rayBody, probe.obj >= 0);
+            }
+            if (o < MAX_MESHES) rayVsMesh(S, o, from, to, hit);
+            else rayVsPlane(S, o, from, to, hit);
         } else {
             int bi = o - OBJ_BALL;
             const Body& b = W.b[bi];

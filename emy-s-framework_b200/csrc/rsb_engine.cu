@@ -20,6 +20,10 @@
 #include "arena_build.h"
 #include "engine_host.h"
 #include "env_kernels.cuh"
+#include "culler.cuh"
+
+#include <numeric>
+#include <random>
 
 using namespace rsb;
 
@@ -101,6 +105,20 @@ struct rsb_handle {
     float* dRewards = nullptr;
     uint8_t* dTerminals = nullptr;
     int32_t* dResetIdx = nullptr;
+    // learned culler
+    int cullMode = RSB_CULL_EXACT;
+    float cullSlack = 0.f;                 // rsb_config.cull_margin: extra uu on top of the calibrated margin
+    bool cullerReady = false;
+    CullParams cullParams{};
+    float* dCw = nullptr;                  // FP32 master weights, Adam moments, gradient (4 x CM_NPARAM)
+    __nv_bfloat16* dCwBf = nullptr;        // BF16 weights used by every forward pass
+    uint32_t* dCull = nullptr;             // per-arena body bits of the current launch
+    unsigned long long* dCounters = nullptr;  // static tests run / culled / culled-but-hit
+    float* dLog = nullptr;                 // logged body centres (uu), for training
+    int64_t logCount = 0, logCap = 0;
+    float* dTris = nullptr;                // mesh triangles in uu (9 floats each)
+    int numTris = 0;
+    std::shared_ptr<ArenaStaticHost> host;
     // launch configuration of the step kernel (indices into kStepVariants / kStepBlocks)
     int stepVariant = 0, stepBlock = 2;
     uint32_t* dScratch = nullptr;   // the autotuner's copy of the arena records
@@ -179,6 +197,9 @@ static EngineView devView(rsb_handle* h) {
     D.arena = h->dArena;
     D.controls = reinterpret_cast<const CtlRec*>(h->dControls);
     D.seed = (uint32_t)(h->seed ^ (h->seed >> 32));
+    D.cull = nullptr;
+    D.cullAudit = h->cullMode == RSB_CULL_LEARNED_AUDIT;
+    D.counters = h->dCounters;
     return D;
 }
 
@@ -261,6 +282,24 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     else defaultMutators(&h->mut);
     computeParams(h->mut, h->P);
     h->obsStride = RSB_OBS_BASE + RSB_OBS_PER_CAR * h->maxCars;
+    if (cfg->cull_mode < RSB_CULL_EXACT || cfg->cull_mode > RSB_CULL_LEARNED_AUDIT)
+        return fail(nullptr, RSB_ERR_INVALID, "unknown cull mode");
+    h->cullMode = cfg->cull_mode;
+    h->cullSlack = cfg->cull_margin;
+    {
+        // reach of each body's static tests around its centre (uu): the car's box and its
+        // four wheel rays, the ball's sphere, each plus its contact-breaking threshold
+        const CarParams& C = h->P.car;
+        float box = length(C.childOff) + length(C.boxHeM);
+        float rays = 0.f;
+        for (int w = 0; w < 4; w++) rays = std::max(rays, length(C.wheelConn[w]) + C.rayLen[w]);
+        CullParams& cp = h->cullParams;
+        cp.carReach = (std::max(box, rays) + C.cbt) * kBtToUu + 10.f;
+        cp.ballReach = (h->P.ballRadius + h->P.ballCbt) * kBtToUu + 10.f;
+        cp.carVmax = 5000.f;   // above the 2300 uu/s clamp: bumps land on top of it within a tick
+        cp.ballVmax = 8000.f;  // above the 6000 uu/s clamp for the same reason
+        cp.dt = h->P.dt;
+    }
     if (!buildEnvTables(h->tables)) return fail(nullptr, RSB_ERR_STATE, "boost pad tables do not match");
     if (cfg->rewards) {
         const rsb_reward_config& r = *cfg->rewards;
@@ -291,6 +330,7 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
         } else {
             H = it->second;
         }
+        h->host = H;
         auto key = std::make_pair(h->device, folder);
         auto dit = c.dev.find(key);
         if (dit != c.dev.end()) {
@@ -344,7 +384,8 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
         !dalloc(h->dObs, (size_t)h->numCars * h->obsStride * 4) ||
         !dalloc(h->dMasks, (size_t)h->numCars * RSB_NUM_ACTIONS) ||
         !dalloc(h->dRewards, (size_t)h->numCars * 4) || !dalloc(h->dTerminals, N) ||
-        !dalloc(h->dResetIdx, N * 4))
+        !dalloc(h->dResetIdx, N * 4) || !dalloc(h->dCull, N * 4) ||
+        !dalloc(h->dCounters, 4 * sizeof(unsigned long long)))
         return fail(nullptr, RSB_ERR_NOMEM, "device allocation failed");
     cudaMemcpy(h->dTeamSize, h->teamSize.data(), N * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(h->dCarOffset, h->carOffset.data(), (N + 1) * 4, cudaMemcpyHostToDevice);
@@ -368,6 +409,8 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dTeamSize); cudaFree(h->dCarOffset); cudaFree(h->dBall); cudaFree(h->dCar);
     cudaFree(h->dPad); cudaFree(h->dArena); cudaFree(h->dControls); cudaFree(h->dLut); cudaFree(h->dActions);
     cudaFree(h->dScratch);
+    cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
+    cudaFree(h->dTris);
     cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -395,8 +438,16 @@ rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
     if (ticks == 0) return RSB_OK;
     RSB_CUDA(cudaSetDevice(h->device));
     EngineView D = devView(h);
+    cudaStream_t st = pick(h, stream);
+    if (h->cullMode != RSB_CULL_EXACT && h->cullerReady) {
+        cullKernel<<<(h->N + 127) / 128, 128, 0, st>>>(h->dCwBf, h->cullParams, h->dBall, h->dCar, h->dArena,
+                                                       h->dTeamSize, h->N, ticks, h->dCull,
+                                                       (int)(offsetof(ArenaP, status) / 4), WS_CULL_MISS);
+        RSB_CUDA(cudaGetLastError());
+        D.cull = h->dCull;
+    }
     int block = kStepBlocks[h->stepBlock], grid = (h->N + block - 1) / block;
-    kStepVariants[h->stepVariant].fn<<<grid, block, 0, pick(h, stream)>>>(D, ticks);
+    kStepVariants[h->stepVariant].fn<<<grid, block, 0, st>>>(D, ticks);
     RSB_CUDA(cudaGetLastError());
     h->stats.ticks_simulated += (uint64_t)h->N * ticks;
     return RSB_OK;
@@ -652,9 +703,344 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
 
 rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out) {
     if (!h || !out) return RSB_ERR_INVALID;
+    RSB_CUDA(cudaSetDevice(h->device));
+    unsigned long long c[4] = {0, 0, 0, 0};
+    RSB_CUDA(cudaMemcpyAsync(c, h->dCounters, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<uint32_t> status;
+    rsb_status st = download(h, h->dArena + (size_t)(offsetof(ArenaP, status) / 4) * h->N, status, h->N);
+    if (st != RSB_OK) return st;
     *out = h->stats;
+    out->narrowphase_queries = c[0];
+    out->culled_queries = c[1];
+    out->missed_contacts = c[2];
+    uint64_t reverted = 0, bits = 0;
+    for (uint32_t v : status) {
+        bits |= v;
+        if (v & WS_CULL_MISS) reverted++;
+    }
+    out->arenas_reverted = reverted;
+    out->status_bits_seen = bits;
     return RSB_OK;
 }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ learned culler
+// (the rsb_culler_* definitions keep the C linkage of their declarations in rsb.h)
+
+__global__ void logCentresKernel(const uint32_t* ball, const uint32_t* car, const int32_t* teamSize,
+                                 const int32_t* carOffset, int N, float* log, int64_t base, int64_t cap) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= N) return;
+    auto put = [&](int64_t i, float x, float y, float z) {
+        if (i < cap) {
+            log[3 * i] = x * kBtToUu;
+            log[3 * i + 1] = y * kBtToUu;
+            log[3 * i + 2] = z * kBtToUu;
+        }
+    };
+    put(base + a, __uint_as_float(ball[a]), __uint_as_float(ball[(size_t)N + a]), __uint_as_float(ball[(size_t)2 * N + a]));
+    for (int s = 0; s < 2 * teamSize[a]; s++)
+        put(base + N + carOffset[a] + s, __uint_as_float(car[((size_t)0 * MAX_CARS + s) * N + a]),
+            __uint_as_float(car[((size_t)1 * MAX_CARS + s) * N + a]),
+            __uint_as_float(car[((size_t)2 * MAX_CARS + s) * N + a]));
+}
+
+constexpr int64_t kCullLogCap = 8 * 1024 * 1024;
+
+static rsb_status ensureCuller(rsb_handle* h) {
+    RSB_CUDA(cudaSetDevice(h->device));
+    if (!h->dCw) {
+        if (cudaMalloc((void**)&h->dCw, 4 * CM_NPARAM * sizeof(float)) != cudaSuccess ||
+            cudaMalloc((void**)&h->dCwBf, CM_NPARAM * sizeof(__nv_bfloat16)) != cudaSuccess)
+            return fail(h, RSB_ERR_NOMEM, "culler weight allocation failed");
+        RSB_CUDA(cudaMemset(h->dCw, 0, 4 * CM_NPARAM * sizeof(float)));
+        RSB_CUDA(cudaFuncSetAttribute(mlpTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM));
+    }
+    if (!h->dTris) {
+        const ArenaStaticHost& H = *h->host;
+        std::vector<float> t;
+        t.reserve(H.triVerts.size() * 3);
+        for (const V3& v : H.triVerts) {
+            t.push_back(v.x * kBtToUu);
+            t.push_back(v.y * kBtToUu);
+            t.push_back(v.z * kBtToUu);
+        }
+        h->numTris = (int)(H.triVerts.size() / 3);
+        if (cudaMalloc((void**)&h->dTris, t.size() * sizeof(float)) != cudaSuccess)
+            return fail(h, RSB_ERR_NOMEM, "triangle allocation failed");
+        RSB_CUDA(cudaMemcpy(h->dTris, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return RSB_OK;
+}
+
+// Device buffer that frees itself.
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    ~DevBuf() { cudaFree(p); }
+    bool alloc(size_t n) { return cudaMalloc((void**)&p, std::max<size_t>(1, n) * sizeof(T)) == cudaSuccess; }
+};
+
+static rsb_status meshDistances(rsb_handle* h, const float* dPts, int64_t n, float* dOut) {
+    for (int64_t i0 = 0; i0 < n; i0 += (1 << 22)) {
+        const int cnt = (int)std::min<int64_t>(n - i0, 1 << 22);
+        meshDistanceKernel<<<(cnt + 255) / 256, 256, 0, h->stream>>>(dPts + 3 * i0, cnt, h->dTris, h->numTris, dOut + i0);
+        RSB_CUDA(cudaGetLastError());
+    }
+    return RSB_OK;
+}
+
+static rsb_status uploadWeights(rsb_handle* h, const float* w) {
+    std::vector<__nv_bfloat16> bf(CM_NPARAM);
+    for (int k = 0; k < CM_NPARAM; k++) bf[k] = __float2bfloat16_rn(w[k]);
+    RSB_CUDA(cudaMemcpy(h->dCw, w, CM_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+    RSB_CUDA(cudaMemcpy(h->dCwBf, bf.data(), CM_NPARAM * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+    return RSB_OK;
+}
+
+rsb_status rsb_culler_log(rsb_handle* h, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    RSB_CUDA(cudaSetDevice(h->device));
+    if (!h->dLog) {
+        if (cudaMalloc((void**)&h->dLog, 3 * kCullLogCap * sizeof(float)) != cudaSuccess)
+            return fail(h, RSB_ERR_NOMEM, "culler log allocation failed");
+        h->logCap = kCullLogCap;
+    }
+    if (h->logCount >= h->logCap) return RSB_OK;
+    logCentresKernel<<<(h->N + 127) / 128, 128, 0, pick(h, stream)>>>(h->dBall, h->dCar, h->dTeamSize, h->dCarOffset,
+                                                                        h->N, h->dLog, h->logCount, h->logCap);
+    RSB_CUDA(cudaGetLastError());
+    h->logCount = std::min<int64_t>(h->logCap, h->logCount + h->N + h->numCars);
+    return RSB_OK;
+}
+
+rsb_status rsb_culler_distance(rsb_handle* h, const float* pts, int32_t n, float* out) {
+    if (!h || n < 0 || (n > 0 && (!pts || !out))) return fail(h, RSB_ERR_INVALID, "bad distance query");
+    rsb_status st = ensureCuller(h);
+    if (st != RSB_OK || n == 0) return st;
+    DevBuf<float> dp, dd;
+    if (!dp.alloc(3 * (size_t)n) || !dd.alloc(n)) return fail(h, RSB_ERR_NOMEM, "distance buffers");
+    RSB_CUDA(cudaMemcpy(dp.p, pts, 12 * (size_t)n, cudaMemcpyHostToDevice));
+    if ((st = meshDistances(h, dp.p, n, dd.p)) != RSB_OK) return st;
+    RSB_CUDA(cudaMemcpyAsync(out, dd.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
+}
+
+rsb_status rsb_culler_predict(rsb_handle* h, const float* pts, int32_t n, float* out) {
+    if (!h || n < 0 || (n > 0 && (!pts || !out))) return fail(h, RSB_ERR_INVALID, "bad predict query");
+    rsb_status st = ensureCuller(h);
+    if (st != RSB_OK || n == 0) return st;
+    DevBuf<float> dp, dd;
+    if (!dp.alloc(3 * (size_t)n) || !dd.alloc(n)) return fail(h, RSB_ERR_NOMEM, "predict buffers");
+    RSB_CUDA(cudaMemcpy(dp.p, pts, 12 * (size_t)n, cudaMemcpyHostToDevice));
+    mlpPredictKernel<<<(n + 255) / 256, 256, 0, h->stream>>>(h->dCwBf, dp.p, n, dd.p);
+    RSB_CUDA(cudaGetLastError());
+    RSB_CUDA(cudaMemcpyAsync(out, dd.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
+}
+
+rsb_status rsb_culler_gradients(rsb_handle* h, const float* pts, const float* target, int32_t n, float over_weight,
+                                float* grad, float* loss) {
+    if (!h || n <= 0 || !pts || !target || !grad) return fail(h, RSB_ERR_INVALID, "bad gradient query");
+    rsb_status st = ensureCuller(h);
+    if (st != RSB_OK) return st;
+    DevBuf<float> dp, dt, dg, dl;
+    if (!dp.alloc(3 * (size_t)n) || !dt.alloc(n) || !dg.alloc(CM_NPARAM) || !dl.alloc(1))
+        return fail(h, RSB_ERR_NOMEM, "gradient buffers");
+    RSB_CUDA(cudaMemcpy(dp.p, pts, 12 * (size_t)n, cudaMemcpyHostToDevice));
+    RSB_CUDA(cudaMemcpy(dt.p, target, 4 * (size_t)n, cudaMemcpyHostToDevice));
+    RSB_CUDA(cudaMemset(dg.p, 0, CM_NPARAM * sizeof(float)));
+    RSB_CUDA(cudaMemset(dl.p, 0, sizeof(float)));
+    mlpTrainKernel<<<(n + TR_TILE - 1) / TR_TILE, TR_TILE, TR_SMEM, h->stream>>>(h->dCwBf, dp.p, dt.p, n, 1.f / n,
+                                                                                 over_weight, dg.p, dl.p);
+    RSB_CUDA(cudaGetLastError());
+    RSB_CUDA(cudaMemcpyAsync(grad, dg.p, CM_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    float l = 0.f;
+    RSB_CUDA(cudaMemcpyAsync(&l, dl.p, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    if (loss) *loss = l;
+    return RSB_OK;
+}
+
+rsb_status rsb_culler_get(rsb_handle* h, float* params, float* margin) {
+    if (!h) return RSB_ERR_INVALID;
+    rsb_status st = ensureCuller(h);
+    if (st != RSB_OK) return st;
+    if (params) RSB_CUDA(cudaMemcpy(params, h->dCw, CM_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    if (margin) *margin = h->cullParams.margin;
+    return RSB_OK;
+}
+
+rsb_status rsb_culler_set(rsb_handle* h, const float* params, float margin) {
+    if (!h || !params || !(margin >= 0.f)) return fail(h, RSB_ERR_INVALID, "bad culler parameters");
+    rsb_status st = ensureCuller(h);
+    if (st != RSB_OK) return st;
+    if ((st = uploadWeights(h, params)) != RSB_OK) return st;
+    h->cullParams.margin = margin + h->cullSlack;
+    h->cullerReady = true;
+    return RSB_OK;
+}
+
+rsb_status rsb_culler_train(rsb_handle* h, const rsb_culler_config* cfg, rsb_culler_report* rep) {
+    if (!h || !cfg || cfg->train_points <= 0 || cfg->heldout_points <= 0 || cfg->epochs <= 0 || cfg->batch <= 0)
+        return fail(h, RSB_ERR_INVALID, "bad culler training configuration");
+    rsb_status st = ensureCuller(h);
+    if (st != RSB_OK) return st;
+    cudaEvent_t t0, t1;
+    RSB_CUDA(cudaEventCreate(&t0));
+    RSB_CUDA(cudaEventCreate(&t1));
+    RSB_CUDA(cudaEventRecord(t0, h->stream));
+    std::mt19937_64 rng(cfg->seed);
+    std::normal_distribution<float> gauss(0.f, 1.f);
+    std::uniform_real_distribution<float> uni(0.f, 1.f);
+    const int64_t total = (int64_t)cfg->train_points + cfg->heldout_points;
+
+    // 1. logged centres and their distances (near-surface ones seed the jittered points)
+    std::vector<float> logged(3 * (size_t)h->logCount), loggedD(h->logCount);
+    if (h->logCount) {
+        RSB_CUDA(cudaStreamSynchronize(h->stream));
+        RSB_CUDA(cudaMemcpy(logged.data(), h->dLog, logged.size() * 4, cudaMemcpyDeviceToHost));
+        DevBuf<float> dd;
+        if (!dd.alloc(h->logCount)) return fail(h, RSB_ERR_NOMEM, "distance buffer");
+        if ((st = meshDistances(h, h->dLog, h->logCount, dd.p)) != RSB_OK) return st;
+        RSB_CUDA(cudaMemcpyAsync(loggedD.data(), dd.p, loggedD.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        RSB_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    std::vector<int64_t> near;
+    for (int64_t i = 0; i < h->logCount; i++)
+        if (loggedD[i] < cfg->near_surface) near.push_back(i);
+
+    // 2. the point set: logged centres, jittered near-surface centres, uniform points
+    std::vector<float> pts(3 * (size_t)total);
+    const float ux = ARENA_EXTENT_X + 200.f, uy = 6100.f, uz = ARENA_HEIGHT + 100.f;
+    for (int64_t i = 0; i < total; i++) {
+        float* p = &pts[3 * i];
+        const float r = uni(rng);
+        if (h->logCount && r < cfg->logged_fraction) {
+            int64_t k = (int64_t)(uni(rng) * h->logCount) % h->logCount;
+            p[0] = logged[3 * k]; p[1] = logged[3 * k + 1]; p[2] = logged[3 * k + 2];
+        } else if (!near.empty() && r < cfg->logged_fraction + cfg->jitter_fraction) {
+            int64_t k = near[(size_t)(uni(rng) * near.size()) % near.size()];
+            for (int c = 0; c < 3; c++) p[c] = logged[3 * k + c] + cfg->jitter_sigma * gauss(rng);
+        } else {
+            p[0] = (2.f * uni(rng) - 1.f) * ux;
+            p[1] = (2.f * uni(rng) - 1.f) * uy;
+            p[2] = -100.f + uni(rng) * uz;
+        }
+    }
+    DevBuf<float> dPts, dDist, dLoss, dPred;
+    if (!dPts.alloc(pts.size()) || !dDist.alloc(total) || !dLoss.alloc(1) || !dPred.alloc(cfg->heldout_points))
+        return fail(h, RSB_ERR_NOMEM, "training buffers");
+    RSB_CUDA(cudaMemcpy(dPts.p, pts.data(), pts.size() * 4, cudaMemcpyHostToDevice));
+    if ((st = meshDistances(h, dPts.p, total, dDist.p)) != RSB_OK) return st;
+    std::vector<float> dist(total);
+    RSB_CUDA(cudaMemcpyAsync(dist.data(), dDist.p, total * 4, cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    // training targets are clamped: the bound only has to be tight where culling is decided
+    std::vector<float> target(dist);
+    for (float& d : target) d = std::min(d, cfg->target_cap);
+    DevBuf<float> dTarget;
+    if (!dTarget.alloc(total)) return fail(h, RSB_ERR_NOMEM, "target buffer");
+    RSB_CUDA(cudaMemcpy(dTarget.p, target.data(), total * 4, cudaMemcpyHostToDevice));
+
+    // 3. initial weights (He-uniform), Adam state cleared
+    std::vector<float> w(CM_NPARAM, 0.f);
+    auto fill = [&](int off, int cnt, int fanIn) {
+        const float b = std::sqrt(6.f / fanIn);
+        for (int k = 0; k < cnt; k++) w[off + k] = (2.f * uni(rng) - 1.f) * b;
+    };
+    fill(CP_W1, 3 * CM_H, 3);
+    fill(CP_W2, CM_H * CM_H, CM_H);
+    fill(CP_W3, CM_H, CM_H);
+    for (int k = 0; k < CM_H; k++) w[CP_B1 + k] = 0.01f;
+    if ((st = uploadWeights(h, w.data())) != RSB_OK) return st;
+    RSB_CUDA(cudaMemset(h->dCw + CM_NPARAM, 0, 3 * CM_NPARAM * sizeof(float)));
+    float* dM = h->dCw + CM_NPARAM;
+    float* dV = dM + CM_NPARAM;
+    float* dG = dV + CM_NPARAM;
+
+    // 4. Adam over shuffled mini-batches of the training part (points are already random)
+    const int64_t ntrain = cfg->train_points;
+    const int bsz = cfg->batch;
+    int steps = 0;
+    float lastLoss = 0.f;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const int stepsPerEpoch = (int)((ntrain + bsz - 1) / bsz);
+    const int totalSteps = stepsPerEpoch * cfg->epochs;
+    for (int ep = 0; ep < cfg->epochs; ep++) {
+        RSB_CUDA(cudaMemsetAsync(dLoss.p, 0, sizeof(float), h->stream));
+        const int64_t shift = (int64_t)(uni(rng) * bsz);  // vary the batch boundaries per epoch
+        for (int64_t b0 = 0; b0 < ntrain; b0 += bsz) {
+            const int64_t start = (b0 + shift) % ntrain;
+            const int cnt = (int)std::min<int64_t>(bsz, ntrain - start);
+            mlpTrainKernel<<<(cnt + TR_TILE - 1) / TR_TILE, TR_TILE, TR_SMEM, h->stream>>>(
+                h->dCwBf, dPts.p + 3 * start, dTarget.p + start, cnt, 1.f / cnt, cfg->over_weight, dG,
+                dLoss.p);
+            steps++;
+            // cosine decay of the learning rate
+            const float lr = cfg->lr * 0.5f * (1.f + std::cos(3.14159265f * (float)steps / (float)totalSteps));
+            const float c1 = 1.f - std::pow(b1, (float)steps), c2 = 1.f - std::pow(b2, (float)steps);
+            adamKernel<<<(CM_NPARAM + 255) / 256, 256, 0, h->stream>>>(h->dCw, dM, dV, dG, h->dCwBf, lr, b1, b2, c1,
+                                                                      c2, 1e-8f);
+        }
+        RSB_CUDA(cudaGetLastError());
+        RSB_CUDA(cudaMemcpyAsync(&lastLoss, dLoss.p, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        RSB_CUDA(cudaStreamSynchronize(h->stream));
+        lastLoss /= (float)stepsPerEpoch;
+    }
+
+    // 5. margin: the largest over-estimate on the held-out points, so that the bound
+    // holds on every one of them
+    const int nh = cfg->heldout_points;
+    mlpPredictKernel<<<(nh + 255) / 256, 256, 0, h->stream>>>(h->dCwBf, dPts.p + 3 * ntrain, nh, dPred.p);
+    RSB_CUDA(cudaGetLastError());
+    std::vector<float> pred(nh);
+    RSB_CUDA(cudaMemcpyAsync(pred.data(), dPred.p, nh * 4, cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaEventRecord(t1, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    double mae = 0.0;
+    float maxOver = 0.f;
+    for (int i = 0; i < nh; i++) {
+        const float d = dist[ntrain + i];
+        mae += std::fabs(std::min(pred[i], cfg->target_cap) - std::min(d, cfg->target_cap));
+        maxOver = std::max(maxOver, pred[i] - d);
+    }
+    const float margin = maxOver + cfg->margin_slack;
+    int misses = 0, clear = 0;
+    const float carNeed = h->cullParams.carReach + h->cullParams.carVmax * 8 * h->P.dt;
+    for (int i = 0; i < nh; i++) {
+        const float b = pred[i] - margin;
+        if (b > dist[ntrain + i]) misses++;
+        if (b >= carNeed) clear++;
+    }
+    h->cullParams.margin = margin + h->cullSlack;
+    h->cullerReady = true;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rep) {
+        *rep = rsb_culler_report{};
+        rep->train_points = cfg->train_points;
+        rep->heldout_points = nh;
+        rep->logged_points = (int32_t)h->logCount;
+        rep->epochs = cfg->epochs;
+        rep->steps = steps;
+        rep->final_loss = lastLoss;
+        rep->margin = margin;
+        rep->heldout_mae = (float)(mae / nh);
+        rep->heldout_max_over = maxOver;
+        rep->heldout_misses = misses;
+        rep->heldout_car_clear = (float)clear / nh;
+        rep->train_ms = ms;
+    }
+    return RSB_OK;
+}
+
+extern "C" {
 
 rsb_status rsb_last_error(const rsb_handle* h, char* buf, size_t n) {
     if (!buf || n == 0) return RSB_ERR_INVALID;

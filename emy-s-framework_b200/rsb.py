@@ -28,7 +28,8 @@ RSB_OBS_BASE = 51
 RSB_OBS_PER_CAR = 29
 
 RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS = range(6)
-RSB_CULL_EXACT, RSB_CULL_LEARNED = 0, 1
+RSB_CULL_EXACT, RSB_CULL_LEARNED, RSB_CULL_LEARNED_AUDIT = 0, 1, 2
+RSB_CULLER_PARAMS = 4481
 RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT = 0, 1, 2
 RSB_ARENA_NONFINITE, RSB_ARENA_ROW_OVERFLOW, RSB_ARENA_BVH_OVERFLOW, RSB_ARENA_CULL_MISS, RSB_ARENA_EPA_OVERFLOW = (
     1, 2, 4, 8, 16)
@@ -123,6 +124,30 @@ class Config(C.Structure):
                 ("device", C.c_int32), ("threads", C.c_int32)]
 
 
+class CullerConfig(C.Structure):
+    _fields_ = [("train_points", C.c_int32), ("heldout_points", C.c_int32), ("logged_fraction", C.c_float),
+                ("jitter_fraction", C.c_float), ("jitter_sigma", C.c_float), ("near_surface", C.c_float),
+                ("target_cap", C.c_float), ("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
+                ("over_weight", C.c_float), ("margin_slack", C.c_float), ("seed", C.c_uint64)]
+
+
+class CullerReport(C.Structure):
+    _fields_ = [("train_points", C.c_int32), ("heldout_points", C.c_int32), ("logged_points", C.c_int32),
+                ("epochs", C.c_int32), ("steps", C.c_int32), ("final_loss", C.c_float), ("margin", C.c_float),
+                ("heldout_mae", C.c_float), ("heldout_max_over", C.c_float), ("heldout_misses", C.c_int32),
+                ("heldout_car_clear", C.c_float), ("train_ms", C.c_float)]
+
+
+def culler_config(**kw) -> CullerConfig:
+    """Defaults of the culler training (4M training and 1M held-out points, 150 uu jitter)."""
+    c = CullerConfig(train_points=4_000_000, heldout_points=1_000_000, logged_fraction=0.45,
+                     jitter_fraction=0.35, jitter_sigma=150.0, near_surface=600.0, target_cap=2500.0,
+                     epochs=30, batch=65536, lr=3e-3, over_weight=4.0, margin_slack=2.0, seed=0x5EED0003)
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
 class TuneEntry(C.Structure):
     _fields_ = [("min_blocks", C.c_int32), ("block", C.c_int32), ("ms", C.c_float)]
 
@@ -158,6 +183,13 @@ _SIGS = {
     "rsb_step": [_P, C.c_int32, _P],
     "rsb_reset_done": [_P, C.c_uint64, C.c_int32, _P],
     "rsb_autotune": [_P, C.c_int32, _P, C.c_int32, _P],
+    "rsb_culler_log": [_P, _P],
+    "rsb_culler_train": [_P, _P, _P],
+    "rsb_culler_get": [_P, _P, _P],
+    "rsb_culler_set": [_P, _P, C.c_float],
+    "rsb_culler_distance": [_P, _P, C.c_int32, _P],
+    "rsb_culler_predict": [_P, _P, C.c_int32, _P],
+    "rsb_culler_gradients": [_P, _P, _P, C.c_int32, C.c_float, _P, _P],
     "rsb_snapshot": [_P, _P],
     "rsb_build_obs": [_P, _P],
     "rsb_build_rewards_terminals": [_P, C.c_int32, _P],
@@ -380,6 +412,47 @@ class Batch:
         n = C.c_int32()
         self._check(self.lib.rsb_autotune(self._h, ticks, out, 32, C.byref(n)))
         return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms} for e in out[:n.value]]
+
+    # ---------------------------------------------------------------- learned culler
+    def culler_log(self, stream: int | None = None):
+        self._check(self.lib.rsb_culler_log(self._h, C.c_void_p(stream or 0)))
+
+    def culler_train(self, cfg: CullerConfig | None = None) -> dict:
+        cfg = cfg or culler_config()
+        rep = CullerReport()
+        self._check(self.lib.rsb_culler_train(self._h, C.byref(cfg), C.byref(rep)))
+        return {n: getattr(rep, n) for n, _ in CullerReport._fields_}
+
+    def culler_get(self):
+        w = np.zeros(RSB_CULLER_PARAMS, np.float32)
+        m = C.c_float()
+        self._check(self.lib.rsb_culler_get(self._h, _ptr(w), C.byref(m)))
+        return w, m.value
+
+    def culler_set(self, params, margin: float):
+        w = np.ascontiguousarray(params, np.float32)
+        self._check(self.lib.rsb_culler_set(self._h, _ptr(w), margin))
+
+    def culler_distance(self, pts) -> np.ndarray:
+        p = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        out = np.zeros(len(p), np.float32)
+        self._check(self.lib.rsb_culler_distance(self._h, _ptr(p), len(p), _ptr(out)))
+        return out
+
+    def culler_predict(self, pts) -> np.ndarray:
+        p = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        out = np.zeros(len(p), np.float32)
+        self._check(self.lib.rsb_culler_predict(self._h, _ptr(p), len(p), _ptr(out)))
+        return out
+
+    def culler_gradients(self, pts, target, over_weight: float = 4.0):
+        p = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(target, np.float32)
+        g = np.zeros(RSB_CULLER_PARAMS, np.float32)
+        loss = C.c_float()
+        self._check(self.lib.rsb_culler_gradients(self._h, _ptr(p), _ptr(t), len(p), over_weight, _ptr(g),
+                                                  C.byref(loss)))
+        return g, loss.value
 
     def sync(self):
         self._check(self.lib.rsb_sync(self._h))

@@ -87,8 +87,11 @@ enum {
 
 /* Arena-narrowphase mode. */
 enum {
-    RSB_CULL_EXACT = 0,   /* every query runs the exact BVH narrowphase */
-    RSB_CULL_LEARNED = 1  /* a learned distance bound skips queries that are provably clear */
+    RSB_CULL_EXACT = 0,         /* every query runs the exact BVH narrowphase */
+    RSB_CULL_LEARNED = 1,       /* a learned distance bound skips the static tests of bodies it
+                                   places clear of every static shape for the launch */
+    RSB_CULL_LEARNED_AUDIT = 2  /* as LEARNED, but the skipped tests run anyway: whatever they find
+                                   counts as a missed contact and reverts the arena to EXACT */
 };
 
 /* Reset modes for rsb_reset_arenas. */
@@ -311,6 +314,56 @@ typedef struct rsb_tune_entry {
  * rsb_step calls, and reports every candidate in out[0..cap).  Allocates the scratch copy
  * of the state on its first call.  No counterpart in the reference. */
 rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32_t cap, int32_t* count);
+
+/* ---- learned culler (no counterpart in the reference) ----
+ * A 3 -> 64 -> 64 -> 1 MLP (BF16 weights, FP32 accumulation) estimates the distance (uu)
+ * from a point to the arena meshes; it is trained on the GPU by the library's own forward /
+ * backward kernels on positions the simulation visits, and its margin is calibrated so that
+ * the estimate minus the margin stays below the exact distance on every held-out point.
+ * With cull_mode LEARNED / LEARNED_AUDIT and trained (or set) weights, every rsb_step first
+ * marks the bodies whose static tests cannot find anything during the launch. */
+#define RSB_CULLER_PARAMS 4481
+
+typedef struct rsb_culler_config {
+    int32_t train_points;     /* points the MLP is fitted on (e.g. 4,000,000) */
+    int32_t heldout_points;   /* further points that calibrate the margin (e.g. 1,000,000) */
+    float logged_fraction;    /* share of points taken from the logged body centres */
+    float jitter_fraction;    /* share of logged near-surface centres moved by Gaussian jitter */
+    float jitter_sigma;       /* uu (e.g. 150) */
+    float near_surface;       /* uu: logged centres closer than this to a mesh get jittered */
+    float target_cap;         /* uu: distances beyond this are clamped in the loss */
+    int32_t epochs;
+    int32_t batch;
+    float lr;                 /* Adam, cosine-decayed */
+    float over_weight;        /* loss weight of over-estimates (they widen the margin) */
+    float margin_slack;       /* uu added to the calibrated margin */
+    uint64_t seed;
+} rsb_culler_config;
+
+typedef struct rsb_culler_report {
+    int32_t train_points, heldout_points, logged_points, epochs, steps;
+    float final_loss;         /* mean weighted squared error (km^2) of the last epoch */
+    float margin;             /* uu subtracted from the estimate */
+    float heldout_mae;        /* uu, mean absolute error (distances capped at target_cap) */
+    float heldout_max_over;   /* uu, largest over-estimate before the margin */
+    int32_t heldout_misses;   /* held-out points where estimate - margin exceeds the exact distance */
+    float heldout_car_clear;  /* share of held-out points whose bound clears a car's 8-tick reach */
+    float train_ms;
+} rsb_culler_report;
+
+/* Appends the centre of every body (ball, cars) to the training log (up to 8M points). */
+rsb_status rsb_culler_log(rsb_handle* h, void* stream);
+/* Builds the point set, computes exact distances, trains, calibrates, and turns the bound on. */
+rsb_status rsb_culler_train(rsb_handle* h, const rsb_culler_config* cfg, rsb_culler_report* out);
+/* FP32 master weights (RSB_CULLER_PARAMS floats) and the calibrated margin (uu). */
+rsb_status rsb_culler_get(rsb_handle* h, float* params, float* margin);
+rsb_status rsb_culler_set(rsb_handle* h, const float* params, float margin);
+/* Host buffers: exact distance to the meshes, the MLP estimate (before the margin), and the
+ * loss gradient of the current weights over n points (the training kernel's reduction). */
+rsb_status rsb_culler_distance(rsb_handle* h, const float* pts, int32_t n, float* out);
+rsb_status rsb_culler_predict(rsb_handle* h, const float* pts, int32_t n, float* out);
+rsb_status rsb_culler_gradients(rsb_handle* h, const float* pts, const float* target, int32_t n,
+                                float over_weight, float* grad, float* loss);
 
 rsb_status rsb_sync(rsb_handle* h);
 rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out);

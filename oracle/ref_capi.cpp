@@ -475,6 +475,15 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
 
 rsb_status rsb_sync(rsb_handle* h) { return h ? RSB_OK : RSB_ERR_INVALID; }
 
+// The learned culler is a GPU component with no CPU counterpart in the reference.
+rsb_status rsb_culler_log(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+rsb_status rsb_culler_train(rsb_handle* h, const rsb_culler_config*, rsb_culler_report*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+rsb_status rsb_culler_get(rsb_handle* h, float*, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+rsb_status rsb_culler_set(rsb_handle* h, const float*, float) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+rsb_status rsb_culler_distance(rsb_handle* h, const float*, int32_t, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+rsb_status rsb_culler_predict(rsb_handle* h, const float*, int32_t, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+rsb_status rsb_culler_gradients(rsb_handle* h, const float*, const float*, int32_t, float, float*, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+
 // The CPU oracle has a single configuration.
 rsb_status rsb_autotune(rsb_handle* h, int32_t, rsb_tune_entry*, int32_t, int32_t* count) {
     if (!h) return RSB_ERR_INVALID;

@@ -28,20 +28,33 @@ def test_golden_file_shapes(pkg):
 
 
 def test_oracle_reproduces_golden(pkg, oracle_lib, meshes_dir):
+    """The reference's car order depends on the heap addresses of its cars, so an arena is
+    checked in a batch where its order matches the recorded one; fresh batches are made
+    until at least 10 of the 12 arenas have been checked."""
     sys.path.insert(0, os.path.join(HERE, "golden"))
     import make_golden as mg
 
     rsb = pkg.rsb
     g = _load()
-    b = rsb.Batch(oracle_lib, len(g["team_sizes"]), team_sizes=g["team_sizes"], meshes_path=meshes_dir, threads=1)
-    b.set_action_lut(np.frombuffer(g["lut"].tobytes(), rsb.CONTROLS_DTYPE))
-    cars = np.frombuffer(g["init_cars"].tobytes(), rsb.CAR_DTYPE).copy()
-    balls = np.frombuffer(g["init_balls"].tobytes(), rsb.BALL_DTYPE).copy()
-    car_kin, car_flags, car_boost, ball_kin = mg.run(b, cars, balls, g["actions"], rsb)
-    same_order = (mg.car_order(b) == g["car_order"]).all(axis=1)
-    assert same_order.sum() >= len(same_order) - 2
-    keep_car = np.repeat(same_order, 2 * g["team_sizes"])
-    assert np.array_equal(car_kin[:, keep_car], g["car_kin"][:, keep_car])
-    assert np.array_equal(car_flags[:, keep_car], g["car_flags"][:, keep_car])
-    assert np.array_equal(car_boost[:, keep_car], g["car_boost"][:, keep_car])
-    assert np.array_equal(ball_kin[:, same_order], g["ball_kin"][:, same_order])
+    verified = np.zeros(len(g["team_sizes"]), bool)
+    keep = []
+    for _ in range(12):
+        b = rsb.Batch(oracle_lib, len(g["team_sizes"]), team_sizes=g["team_sizes"], meshes_path=meshes_dir,
+                      threads=1)
+        keep.append(b)  # distinct heap addresses for the next batch's cars
+        same = (mg.car_order(b) == g["car_order"]).all(axis=1) & ~verified
+        if not same.any():
+            continue
+        b.set_action_lut(np.frombuffer(g["lut"].tobytes(), rsb.CONTROLS_DTYPE))
+        cars = np.frombuffer(g["init_cars"].tobytes(), rsb.CAR_DTYPE).copy()
+        balls = np.frombuffer(g["init_balls"].tobytes(), rsb.BALL_DTYPE).copy()
+        car_kin, car_flags, car_boost, ball_kin = mg.run(b, cars, balls, g["actions"], rsb)
+        keep_car = np.repeat(same, 2 * g["team_sizes"])
+        assert np.array_equal(car_kin[:, keep_car], g["car_kin"][:, keep_car])
+        assert np.array_equal(car_flags[:, keep_car], g["car_flags"][:, keep_car])
+        assert np.array_equal(car_boost[:, keep_car], g["car_boost"][:, keep_car])
+        assert np.array_equal(ball_kin[:, same], g["ball_kin"][:, same])
+        verified |= same
+        if verified.sum() >= 10:
+            break
+    assert verified.sum() >= 10, verified

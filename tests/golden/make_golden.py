@@ -94,7 +94,18 @@ def main():
     rsb = load_pkg().rsb
     lib = rsb.load_library(ORACLE_LIB)
     pkg = load_pkg()
-    batch = rsb.Batch(lib, len(TEAM_SIZES), team_sizes=TEAM_SIZES, meshes_path=pkg.MESHES_DIR, threads=1)
+    # the reference visits an arena's cars in the order of its pointer set; record a batch in
+    # which every arena visits them in reverse creation order (the engine's order)
+    kept, batch = [], None
+    for _ in range(200):
+        b = rsb.Batch(lib, len(TEAM_SIZES), team_sizes=TEAM_SIZES, meshes_path=pkg.MESHES_DIR, threads=1)
+        order = car_order(b)
+        if all(np.array_equal(order[a, :2 * t], np.arange(2 * t)[::-1]) for a, t in enumerate(TEAM_SIZES)):
+            batch = b
+            break
+        kept.append(b)  # keep it alive so the next batch's cars get other addresses
+    if batch is None:
+        raise RuntimeError("no batch with every arena in reverse creation order")
     lut = rsb.default_action_lut(lib)
     batch.set_action_lut(lut)
     cars, balls = initial_state(rsb, batch)

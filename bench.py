@@ -125,6 +125,22 @@ class Workload:
 
 # ------------------------------------------------------------------ our arm
 
+def train_culler(batch, rsb, wl, rank):
+    """Untimed: log body centres from short rollouts of this workload (random-state and
+    high-contact starts), then train and calibrate the culler on the GPU."""
+    rng = np.random.default_rng(0x5EED0005 + rank)
+    t0 = time.perf_counter()
+    for k in range(6):
+        batch.reset_all(0x5EED3000 + k, rsb.RSB_RESET_RANDOM_STATE if k % 3 else rsb.RSB_RESET_HIGH_CONTACT)
+        for _ in range(3):
+            batch.set_actions(rng.integers(0, rsb.RSB_NUM_ACTIONS, batch.num_cars).astype(np.int32))
+            batch.step(wl.tick_skip)
+            batch.culler_log()
+    rep = batch.culler_train(rsb.culler_config())
+    rep["wall_s"] = time.perf_counter() - t0
+    return rep
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -135,15 +151,15 @@ def run_ours(args, rank, world, dist):
     wl = Workload(args)
     rewards = rsb.default_rewards(pkg.engine_library(), episode_max_ticks=EPISODE_TICKS)
     batch = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size,
-                      meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank, rewards=rewards)
-    batch.reset_all(0x5EED0001 + rank, rsb.RSB_RESET_RANDOM_STATE)
+                      meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank, rewards=rewards,
+                      cull_mode=rsb.RSB_CULL_EXACT)
     batch.set_action_lut(rsb.default_action_lut(batch.lib))
+    culler = train_culler(batch, rsb, wl, rank) if args.cull == "learned" else None
 
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     gen = torch.Generator(device=f"cuda:{dev}")
-    gen.manual_seed(0x5EED0003 + rank)
     n_cars = max(1, batch.num_cars)
     actions = torch.empty(n_cars, dtype=torch.int32, device=dev)
     counter = [0]
@@ -163,37 +179,79 @@ def run_ours(args, rank, world, dist):
         counter[0] += 1
         batch.reset_done(0x5EED1000 + counter[0], rsb.RSB_RESET_RANDOM_STATE, stream=sp)
 
+    def start(mode):
+        # every path starts from the same seeded state and action stream
+        batch.set_cull_mode(mode)
+        batch.reset_all(0x5EED0001 + rank, rsb.RSB_RESET_RANDOM_STATE)
+        gen.manual_seed(0x5EED0003 + rank)
+        counter[0] = 0
+
+    def timed(clocks_out):
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                one_step()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        s0 = batch.stats()
+        times, step_times = [], []
+        with ClockSampler(dev) as clocks, torch.cuda.stream(stream):
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                flush.fill_(1.0)  # evict the L2 between timed steps
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                e0.record(stream)
+                one_step(ev)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                step_times.append(ev[0].elapsed_time(ev[1]))
+            torch.cuda.synchronize()
+        clocks_out.append(clocks.summary())
+        s1 = batch.stats()
+        total_ms = float(sum(times))
+        if dist is not None:
+            t = torch.tensor([total_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+            dist.barrier()
+        value = wl.num_arenas * wl.tick_skip * args.steps * world / (total_ms / 1e3)
+        queries = {k: s1[k] - s0[k] for k in ("narrowphase_queries", "culled_queries", "missed_contacts")}
+        return value, total_ms, step_times, queries
+
+    # exact-BVH path (also picks the step kernel's launch configuration)
+    clocks = []
+    start(rsb.RSB_CULL_EXACT)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             one_step()
     torch.cuda.synchronize()
-    # pick the step kernel's launch configuration on a copy of the warmed-up state
     tune = batch.autotune(wl.tick_skip) if not args.no_autotune else []
-    if dist is not None:
-        dist.barrier()
-    times, step_times = [], []
-    with ClockSampler(dev) as clocks, torch.cuda.stream(stream):
+    start(rsb.RSB_CULL_EXACT)
+    ex_value, ex_ms, ex_steps, ex_q = timed(clocks)
+    value, total_ms, step_times, queries = ex_value, ex_ms, ex_steps, ex_q
+    learned = None
+    if culler is not None:
+        start(rsb.RSB_CULL_LEARNED)
+        value, total_ms, step_times, queries = timed(clocks)
+        # the same run once more with the skipped tests executed and checked
+        start(rsb.RSB_CULL_LEARNED_AUDIT)
+        s0 = batch.stats()
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup + args.steps):
+                one_step()
         torch.cuda.synchronize()
-        for _ in range(args.steps):
-            flush.fill_(1.0)  # evict the L2 between timed steps
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            e0.record(stream)
-            one_step(ev)
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
-            step_times.append(ev[0].elapsed_time(ev[1]))
-        torch.cuda.synchronize()
-    total_ms = float(sum(times))
-    if dist is not None:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
-    arena_ticks = wl.num_arenas * wl.tick_skip * args.steps * world
-    value = arena_ticks / (total_ms / 1e3)
+        s1 = batch.stats()
+        tested = queries["culled_queries"] + queries["narrowphase_queries"]
+        learned = {"train": culler, "culled_fraction": queries["culled_queries"] / max(1, tested),
+                   "static_tests": queries, "audit_missed_contacts": s1["missed_contacts"] - s0["missed_contacts"],
+                   "audit_arenas_reverted": s1["arenas_reverted"],
+                   "exact_bvh": {"value": ex_value, "ms_per_step": ex_ms / args.steps,
+                                 "kernel_ms": statistics.mean(ex_steps), "static_tests": ex_q},
+                   "learned_over_exact": value / ex_value}
+        batch.set_cull_mode(rsb.RSB_CULL_LEARNED)
 
     # e2e through the public API with host buffers, as the collector's host path runs it:
     # host actions in (H2D), step, obs / masks / rewards / terminals back to the host (D2H),
@@ -223,21 +281,26 @@ def run_ours(args, rank, world, dist):
     kernel_s = statistics.mean(step_times) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / kernel_s / 1e9
+    cfg = wl.config() | {"parallelism": f"arena-shards x{world}"}
+    if learned is not None:
+        cfg["narrowphase"] = "learned cull (exact BVH for every body the bound does not clear)"
     res = {
         "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random states)",
-        "config": wl.config() | {"parallelism": f"arena-shards x{world}"},
+        "config": cfg,
         "roofline": {"bound": "hbm", "kernel": "stepKernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                      "bytes_per_launch": alg_bytes, "kernel_ms": kernel_s * 1e3,
                      "kernel_share": statistics.mean(step_times) / (total_ms / args.steps)},
         "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": int(statistics.mean(h2d)),
                 "d2h_bytes_per_step": int(statistics.mean(d2h))},
-        # per env step: action expansion, step, obs + masks, rewards + terminals, reset
-        "gpu_launches": args.steps * 5,
+        # per env step: action expansion, (culler,) step, obs + masks, rewards + terminals, reset
+        "gpu_launches": args.steps * (6 if learned is not None else 5),
+        "learned_cull": learned,
         "autotune": tune,
-        "clocks": clocks.summary(),
+        "clocks": clocks[-1],
+        "clocks_exact": clocks[0],
     }
     return res
 
@@ -300,6 +363,7 @@ def main():
     ap.add_argument("--tick-skip", type=int, default=8)
     ap.add_argument("--workload-name", default=None)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--cull", default="learned", choices=["learned", "exact"])
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

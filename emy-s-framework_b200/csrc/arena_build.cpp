@@ -442,12 +442,51 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
 
     S.triInfo = out.triInfo.data();
     S.bpCells = out.bpCells.data();
+
+    // ---- mesh occupancy grid (see ArenaStatic::occ): 64 uu voxels over the arena
+    {
+        const float cell = 64.f * kUuToBt, tol = 2.f * kUuToBt;
+        const V3 gmn = V3{-4400.f, -6300.f, -200.f} * kUuToBt, gmx = V3{4400.f, 6300.f, 2300.f} * kUuToBt;
+        S.occMin = gmn;
+        S.occInvCell = 1.f / cell;
+        S.occX = (int)std::ceil((gmx.x - gmn.x) / cell);
+        S.occY = (int)std::ceil((gmx.y - gmn.y) / cell);
+        S.occZ = (int)std::ceil((gmx.z - gmn.z) / cell);
+        const size_t nv = (size_t)S.occX * S.occY * S.occZ;
+        out.occ.assign((nv + 31) / 32, 0u);
+        const float halfDiag = 0.5f * cell * std::sqrt(3.f);
+        const size_t ntri = out.triVerts.size() / 3;
+        for (size_t t = 0; t < ntri; t++) {
+            const V3 a = out.triVerts[3 * t], b = out.triVerts[3 * t + 1], c = out.triVerts[3 * t + 2];
+            const V3 mn = vmin(vmin(a, b), c) - V3{tol, tol, tol}, mx = vmax(vmax(a, b), c) + V3{tol, tol, tol};
+            V3 n = cross(b - a, c - a);
+            const float nl = std::sqrt(dot(n, n));
+            const bool flat = nl > 0.f;
+            if (flat) n = n * (1.f / nl);
+            auto idx = [&](float v, float o, int hi) {
+                int i = (int)std::floor((v - o) / cell);
+                return i < 0 ? 0 : (i >= hi ? hi - 1 : i);
+            };
+            for (int x = idx(mn.x, gmn.x, S.occX); x <= idx(mx.x, gmn.x, S.occX); x++)
+                for (int y = idx(mn.y, gmn.y, S.occY); y <= idx(mx.y, gmn.y, S.occY); y++)
+                    for (int z = idx(mn.z, gmn.z, S.occZ); z <= idx(mx.z, gmn.z, S.occZ); z++) {
+                        const V3 centre = gmn + V3{(x + 0.5f) * cell, (y + 0.5f) * cell, (z + 0.5f) * cell};
+                        // the triangle's plane must come within the voxel's half diagonal
+                        if (flat && std::fabs(dot(n, centre - a)) > halfDiag + tol) continue;
+                        const size_t v = ((size_t)x * S.occY + y) * S.occZ + z;
+                        out.occ[v >> 5] |= 1u << (v & 31);
+                    }
+        }
+        S.occ = out.occ.data();
+    }
     return true;
 }
 
 ArenaStatic deviceView(const ArenaStaticHost& h, const BvhNode* nodes, const BvhSubtree* subs,
-                       const V3* triVerts, const TriEdgeInfo* triInfo, const uint32_t* bpCells) {
+                       const V3* triVerts, const TriEdgeInfo* triInfo, const uint32_t* bpCells,
+                       const uint32_t* occ) {
     ArenaStatic v = h.view;
+    v.occ = occ;
     v.nodes = nodes;
     v.subs = subs;
     v.triVerts = triVerts;

@@ -19,6 +19,18 @@
 
 namespace rsb {
 
+// Dynamic bodies in ascending (registration stamp, body index) order with their
+// broadphase cells.  btRSBroadphase visits the proxies of a cell in registration order;
+// registrations change only in updateBodyAabb, so the order is rebuilt after it (for the
+// pair search) and before the car pre-ticks (for the wheel rays), which lets both walk it
+// once instead of searching for the next stamp body by body.
+struct RegOrder {
+    int n;
+    int8_t body[MAX_BODIES];
+    uint32_t stamp[MAX_BODIES];
+    int16_t ci[MAX_BODIES], cj[MAX_BODIES], ck[MAX_BODIES];
+};
+
 struct World {
     const ArenaStatic* S;
     const WorldParams* P;
@@ -46,10 +58,16 @@ struct World {
     int32_t cullAudit;
     mutable uint32_t nStatic, nCulled, nMissed;  // static tests run / skipped / skipped but hit
     mutable uint32_t cullMissed;                 // WS_CULL_MISS once a skipped test would have hit
+    RegOrder reg;
 };
 
 // world status bits (per-arena status word)
 enum : uint32_t { WS_NONFINITE = 1u, WS_OVERFLOW = 2u, WS_BVH_OVERFLOW = 4u, WS_CULL_MISS = 8u, WS_EPA_OVERFLOW = 16u };
+
+// Tolerances of the exact query rejects (Bullet units): the occupancy lookup around a mesh
+// query box or ray segment, and the AABB reject before a ray's convex cast.
+constexpr float kOccTol = 2.f * kUuToBt;
+constexpr float kCastTol = 0.1f;
 
 // Bookkeeping of one static test of body b: returns true when the test must be skipped.
 // (nCulled counts the tests the bound clears, also in audit mode where they still run.)
@@ -189,9 +207,38 @@ RSB_HD bool inRegNeighbourhood(const Body& b, int ci, int cj, int ck) {
     return ci >= b.ci - 1 && ci <= b.ci + 1 && cj >= b.cj - 1 && cj <= b.cj + 1 && ck >= b.ck - 1 && ck <= b.ck + 1;
 }
 
+RSB_HD void buildRegOrder(World& W) {
+    RegOrder& R = W.reg;
+    R.n = 0;
+    for (int e = 0; e < W.nb; e++) {
+        const Body& b = W.b[e];
+        // insertion keeps equal stamps in body-index order
+        int r = R.n++;
+        while (r > 0 && R.stamp[r - 1] > b.regStamp) {
+            R.body[r] = R.body[r - 1];
+            R.stamp[r] = R.stamp[r - 1];
+            R.ci[r] = R.ci[r - 1];
+            R.cj[r] = R.cj[r - 1];
+            R.ck[r] = R.ck[r - 1];
+            r--;
+        }
+        R.body[r] = (int8_t)e;
+        R.stamp[r] = b.regStamp;
+        R.ci[r] = (int16_t)b.ci;
+        R.cj[r] = (int16_t)b.cj;
+        R.ck[r] = (int16_t)b.ck;
+    }
+}
+
+RSB_HD bool regNear(const RegOrder& R, int r, int ci, int cj, int ck) {
+    return ci >= R.ci[r] - 1 && ci <= R.ci[r] + 1 && cj >= R.cj[r] - 1 && cj <= R.cj[r] + 1 && ck >= R.ck[r] - 1 &&
+           ck <= R.ck[r] + 1;
+}
+
 // btRSBroadphase::calculateOverlappingPairs
 RSB_HD void computePairs(World& W) {
     W.np = 0;
+    buildRegOrder(W);
     const ArenaStatic& S = *W.S;
     const BpGrid& g = S.bp;
     for (int bi = 0; bi < W.nb; bi++) {
@@ -209,23 +256,20 @@ RSB_HD void computePairs(World& W) {
             int ci = b.cell / (g.cellsY * g.cellsZ);
             int cj = (b.cell / g.cellsZ) % g.cellsY;
             int ck = b.cell % g.cellsZ;
+            const RegOrder& R = W.reg;
             int inCell = 0;
-            for (int e = 0; e < W.nb; e++) inCell += inRegNeighbourhood(W.b[e], ci, cj, ck) ? 1 : 0;
+            for (int r = 0; r < R.n; r++) inCell += regNear(R, r, ci, cj, ck) ? 1 : 0;
             if (inCell > 1) {
-                // visit the other dynamic proxies of this cell in registration order
+                // visit the other dynamic proxies of this cell in registration order (a
+                // proxy whose stamp equals the one just visited is passed over)
                 uint32_t last = 0;
                 bool first = true;
-                for (int it = 0; it < W.nb; it++) {
-                    int pick = -1;
-                    uint32_t best = 0xffffffffu;
-                    for (int e = 0; e < W.nb; e++) {
-                        if (!inRegNeighbourhood(W.b[e], ci, cj, ck)) continue;
-                        uint32_t st = W.b[e].regStamp;
-                        if ((first || st > last) && st < best) { best = st; pick = e; }
-                    }
-                    if (pick < 0) break;
+                for (int r = 0; r < R.n; r++) {
+                    if (!regNear(R, r, ci, cj, ck)) continue;
+                    if (!first && R.stamp[r] <= last) continue;
                     first = false;
-                    last = best;
+                    last = R.stamp[r];
+                    const int pick = R.body[r];
                     if (pick == bi) continue;
                     if (aabbOverlap(b.bpMin, b.bpMax, W.b[pick].bpMin, W.b[pick].bpMax))
                         addPair(W, obj, OBJ_BALL + pick);
@@ -347,6 +391,8 @@ RSB_HD void collideBallMesh(World& W, int mesh, Manifold& man) {
     V3 amn, amx;
     ballAabb(P, ball.xf, amn, amx);  // convexInTriangleSpace == ball transform (mesh at identity)
     M3 invB = inverse(ball.xf.b);
+    // no triangle near the query box: the walk below could not report one
+    if (occAny(*W.S, amn - V3{kOccTol, kOccTol, kOccTol}, amx + V3{kOccTol, kOccTol, kOccTol}))
     bvhQueryAabb(*W.S, mesh, amn, amx, [&](int tri) {
         V3 v[3];
         triVerts(*W.S, mesh, tri, v);
@@ -535,7 +581,8 @@ RSB_HD void collideBoxMesh(World& W, int mesh, int ci, const Xf& childXf, Manifo
     float maxDist2 = sq((C.boxMargin + 0.f) + man.cbt);
     bool responds = carResponds(W, ci);
     bool found = false;
-    if (!cullSkip(W, 1 + ci)) {
+    if (!cullSkip(W, 1 + ci) &&
+        occAny(*W.S, amn - V3{kOccTol, kOccTol, kOccTol}, amx + V3{kOccTol, kOccTol, kOccTol})) {
     bvhQueryAabb(*W.S, mesh, amn, amx, [&](int tri) {
         V3 v[3];
         triVerts(*W.S, mesh, tri, v);
@@ -715,9 +762,13 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
     hit.obj = -1;
     hit.normal = v3zero();
     const int rayBody = ignoreObj - OBJ_BALL;  // the casting car's body
+    // no mesh triangle near the segment: no mesh can be hit
+    const V3 tolv{kOccTol, kOccTol, kOccTol};
+    const bool meshNear = occAny(S, vmin(from, to) - tolv, vmax(from, to) + tolv);
     auto testObj = [&](int o) {
         if (hit.fraction == 0.f) return;
         if (o == ignoreObj) return;
+        if (o < MAX_MESHES && !meshNear) return;
         if (o < NUM_STATICS) {
             if (cullSkip(W, rayBody)) return;
             if ((W.cull >> rayBody) & 1u) {
@@ -744,6 +795,12 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
                 sh = carBoxShape(P.car);
                 x = carChildXf(P.car, b.xf);
             }
+            // a segment that stays clear of the shape's AABB (widened well beyond the cast's
+            // convergence distance) cannot be reported as a hit
+            V3 smn, smx;
+            shapeAabb(sh, x, smn, smx);
+            const V3 pad{kCastTol, kCastTol, kCastTol};
+            if (!aabbOverlap(vmin(from, to), vmax(from, to), smn - pad, smx + pad)) return;
             float frac;
             V3 n;
             if (subsimplexCast(from, to, sh, x, frac, n)) {
@@ -764,20 +821,17 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
         uint32_t mask = S.bpCells[cell];
         for (int s = 0; s < NUM_STATICS; s++)
             if (mask & (1u << s)) testObj(s);
+        // dynamic proxies of the cell in registration order (W.reg is built before the
+        // car pre-ticks; see RegOrder)
+        const RegOrder& R = W.reg;
         uint32_t last = 0;
         bool first = true;
-        for (int it = 0; it < W.nb; it++) {
-            int pick = -1;
-            uint32_t best = 0xffffffffu;
-            for (int e = 0; e < W.nb; e++) {
-                if (!inRegNeighbourhood(W.b[e], i, j, k)) continue;
-                uint32_t st = W.b[e].regStamp;
-                if ((first || st > last) && st < best) { best = st; pick = e; }
-            }
-            if (pick < 0) break;
+        for (int r = 0; r < R.n; r++) {
+            if (!regNear(R, r, i, j, k)) continue;
+            if (!first && R.stamp[r] <= last) continue;
             first = false;
-            last = best;
-            testObj(OBJ_BALL + pick);
+            last = R.stamp[r];
+            testObj(OBJ_BALL + R.body[r]);
         }
     } else {
         for (int o = 0; o < OBJ_BALL + W.nb; o++) testObj(o);

@@ -43,6 +43,7 @@ struct DevStatic {
     V3* triVerts = nullptr;
     TriEdgeInfo* triInfo = nullptr;
     uint32_t* bpCells = nullptr;
+    uint32_t* occ = nullptr;
     ArenaStatic view{};
 };
 
@@ -344,9 +345,9 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
                 return cudaMemcpy(dst, v.data(), bytes, cudaMemcpyHostToDevice) == cudaSuccess;
             };
             if (!up(D->nodes, H->nodes) || !up(D->subs, H->subs) || !up(D->triVerts, H->triVerts) ||
-                !up(D->triInfo, H->triInfo) || !up(D->bpCells, H->bpCells))
+                !up(D->triInfo, H->triInfo) || !up(D->bpCells, H->bpCells) || !up(D->occ, H->occ))
                 return fail(nullptr, RSB_ERR_CUDA, "uploading arena meshes failed");
-            D->view = deviceView(*H, D->nodes, D->subs, D->triVerts, D->triInfo, D->bpCells);
+            D->view = deviceView(*H, D->nodes, D->subs, D->triVerts, D->triInfo, D->bpCells, D->occ);
             c.dev[key] = D;
             h->stat = D;
         }
@@ -862,6 +863,12 @@ rsb_status rsb_culler_gradients(rsb_handle* h, const float* pts, const float* ta
     RSB_CUDA(cudaMemcpyAsync(&l, dl.p, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     RSB_CUDA(cudaStreamSynchronize(h->stream));
     if (loss) *loss = l;
+    return RSB_OK;
+}
+
+rsb_status rsb_set_cull_mode(rsb_handle* h, int32_t mode) {
+    if (!h || mode < RSB_CULL_EXACT || mode > RSB_CULL_LEARNED_AUDIT) return fail(h, RSB_ERR_INVALID, "unknown cull mode");
+    h->cullMode = mode;
     return RSB_OK;
 }
 

@@ -184,6 +184,7 @@ _SIGS = {
     "rsb_reset_done": [_P, C.c_uint64, C.c_int32, _P],
     "rsb_autotune": [_P, C.c_int32, _P, C.c_int32, _P],
     "rsb_culler_log": [_P, _P],
+    "rsb_set_cull_mode": [_P, C.c_int32],
     "rsb_culler_train": [_P, _P, _P],
     "rsb_culler_get": [_P, _P, _P],
     "rsb_culler_set": [_P, _P, C.c_float],
@@ -414,6 +415,9 @@ class Batch:
         return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms} for e in out[:n.value]]
 
     # ---------------------------------------------------------------- learned culler
+    def set_cull_mode(self, mode: int):
+        self._check(self.lib.rsb_set_cull_mode(self._h, mode))
+
     def culler_log(self, stream: int | None = None):
         self._check(self.lib.rsb_culler_log(self._h, C.c_void_p(stream or 0)))
 

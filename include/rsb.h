@@ -355,6 +355,8 @@ typedef struct rsb_culler_report {
 rsb_status rsb_culler_log(rsb_handle* h, void* stream);
 /* Builds the point set, computes exact distances, trains, calibrates, and turns the bound on. */
 rsb_status rsb_culler_train(rsb_handle* h, const rsb_culler_config* cfg, rsb_culler_report* out);
+/* Switches between RSB_CULL_EXACT / _LEARNED / _LEARNED_AUDIT for later rsb_step calls. */
+rsb_status rsb_set_cull_mode(rsb_handle* h, int32_t mode);
 /* FP32 master weights (RSB_CULLER_PARAMS floats) and the calibrated margin (uu). */
 rsb_status rsb_culler_get(rsb_handle* h, float* params, float* margin);
 rsb_status rsb_culler_set(rsb_handle* h, const float* params, float margin);

@@ -476,6 +476,7 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
 rsb_status rsb_sync(rsb_handle* h) { return h ? RSB_OK : RSB_ERR_INVALID; }
 
 // The learned culler is a GPU component with no CPU counterpart in the reference.
+rsb_status rsb_set_cull_mode(rsb_handle* h, int32_t mode) { return mode == RSB_CULL_EXACT ? RSB_OK : fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 rsb_status rsb_culler_log(rsb_handle* h, void*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 rsb_status rsb_culler_train(rsb_handle* h, const rsb_culler_config*, rsb_culler_report*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 rsb_status rsb_culler_get(rsb_handle* h, float*, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }

@@ -107,7 +107,7 @@ RSB_HD void arenaTick(ArenaSim& A) {
     bool ballOnly = W.nc == 0;
     // Arena::_cars is an unordered_set of car pointers: with each car in its own hash
     // bucket, libstdc++ iterates it in reverse insertion order
-    buildRegOrder(W);  // the wheel rays walk the cell proxies in registration order
+    buildRayOrder(W);  // the wheel rays walk the cell proxies in registration order
     for (int ci = W.nc - 1; ci >= 0; ci--) carPreTick(W, ci, mixHash(A.rngKey, (uint32_t)A.tickCount, (uint32_t)ci));
     if (!ballOnly) {
         for (int p = 0; p < NUM_PADS; p++) {

@@ -342,6 +342,7 @@ RSB_HD void carRespawn(World& W, int ci, int pick) {
     // Angle(yaw, 0, 0).ToRotMat() = setEulerYPR(yaw, -0, -0) = setEulerZYX(-0, -0, yaw)
     M3 rot = m3fromEulerZYX(-0.f, -0.f, yaw);
     carSetSpawnState(W, ci, pos, rot, W.P->car.spawnBoost);
+    refreshCastBox(W, 1 + ci);  // the later wheel rays of this tick see the car at its spawn
 }
 
 // Car::_UpdateWheels (Car.cpp:323-461)

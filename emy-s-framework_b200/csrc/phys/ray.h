@@ -61,6 +61,13 @@ RSB_HD void rayVsMesh(const ArenaStatic& S, int mesh, V3 from, V3 to, RayHit& hi
 RSB_HD void rayVsPlane(const ArenaStatic& S, int plane, V3 fromW, V3 toW, RayHit& hit) {
     V3 origin = S.planeOrigin[plane - MAX_MESHES];
     V3 n = S.planeNormal[plane - MAX_MESHES];
+    {
+        // a segment that stays on one side of the plane, farther than any rounding of the
+        // two triangles below from it, crosses neither of them
+        const float tol = 1e-3f;
+        const float sa = dot(n, fromW - origin), sb = dot(n, toW - origin);
+        if ((sa > tol && sb > tol) || (sa < -tol && sb < -tol)) return;
+    }
     // world -> plane-object transform (identity basis): translate by -origin
     Xf inv = xfInverse(Xf{m3identity(), origin});
     V3 from = xfPoint(inv, fromW), to = xfPoint(inv, toW);

@@ -29,6 +29,9 @@ struct RegOrder {
     int8_t body[MAX_BODIES];
     uint32_t stamp[MAX_BODIES];
     int16_t ci[MAX_BODIES], cj[MAX_BODIES], ck[MAX_BODIES];
+    // per body (index = body): the AABB of the shape a wheel ray is cast against, widened
+    // by kCastTol; filled for the car pre-ticks, during which no body moves
+    V3 castMin[MAX_BODIES], castMax[MAX_BODIES];
 };
 
 struct World {
@@ -748,6 +751,25 @@ RSB_HD void dispatchPairs(World& W) {
 
 // ------------------------------------------------------------------ wheel ray casts
 
+// The widened AABB of the shape body bi's wheel-ray tests are cast against (bodies move
+// during the car pre-ticks only when a demolished car respawns, which refreshes its box).
+RSB_HD void refreshCastBox(World& W, int bi) {
+    const WorldParams& P = *W.P;
+    const Body& b = W.b[bi];
+    const V3 pad{kCastTol, kCastTol, kCastTol};
+    V3 mn, mx;
+    if (bi == 0) shapeAabb(makeSphere(P.ballRadius), b.xf, mn, mx);
+    else shapeAabb(carBoxShape(P.car), carChildXf(P.car, b.xf), mn, mx);
+    W.reg.castMin[bi] = mn - pad;
+    W.reg.castMax[bi] = mx + pad;
+}
+
+// Registration order plus the cast boxes, before the car pre-ticks.
+RSB_HD void buildRayOrder(World& W) {
+    buildRegOrder(W);
+    for (int bi = 0; bi < W.nb; bi++) refreshCastBox(W, bi);
+}
+
 // btDefaultVehicleRaycaster::castRay (btDefaultVehicleRaycaster.cpp:32-53) over
 // btCollisionWorld::rayTest with ClosestRayResultCallback ignoring the casting chassis.
 // The broadphase hands over every object registered in the cell of the ray start
@@ -785,6 +807,9 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
             else rayVsPlane(S, o, from, to, hit);
         } else {
             int bi = o - OBJ_BALL;
+            // a segment that stays clear of the shape's AABB (widened well beyond the cast's
+            // convergence distance) cannot be reported as a hit
+            if (!aabbOverlap(vmin(from, to), vmax(from, to), W.reg.castMin[bi], W.reg.castMax[bi])) return;
             const Body& b = W.b[bi];
             ConvexShape sh;
             Xf x;
@@ -795,12 +820,6 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
                 sh = carBoxShape(P.car);
                 x = carChildXf(P.car, b.xf);
             }
-            // a segment that stays clear of the shape's AABB (widened well beyond the cast's
-            // convergence distance) cannot be reported as a hit
-            V3 smn, smx;
-            shapeAabb(sh, x, smn, smx);
-            const V3 pad{kCastTol, kCastTol, kCastTol};
-            if (!aabbOverlap(vmin(from, to), vmax(from, to), smn - pad, smx + pad)) return;
             float frac;
             V3 n;
             if (subsimplexCast(from, to, sh, x, frac, n)) {

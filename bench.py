@@ -100,27 +100,93 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-# ------------------------------------------------------------------ workload
+# ------------------------------------------------------------------ workloads
+
+# The measured configurations (team sizes, arena counts, starts, action distribution and
+# culling of the four GPU workloads; c3 is the headline: learned cull vs exact BVH).
+PRESETS = {
+    "c3": dict(arenas=65536, team=3, mixed=False, reset="random", bias=False, cull="learned", graph=False,
+               desc="soccar 3v3 x 65536 arenas"),
+    "c1": dict(arenas=8192, team=2, mixed=False, reset="random", bias=False, cull="exact", graph=False,
+               desc="soccar 2v2 x 8192 arenas"),
+    "c2": dict(arenas=32768, team=0, mixed=True, reset="random", bias=False, cull="exact", graph=True,
+               desc="mixed 32768 arenas (1v1:2v2:3v3 = 1:1:1) in one launch, env step replayed as a CUDA graph"),
+    "c4": dict(arenas=131072, team=1, mixed=False, reset="high_contact", bias=True, cull="learned", graph=False,
+               desc="soccar 1v1 x 131072 arenas, high-contact starts, boost/jump-biased actions, 4096-tick rollout"),
+}
+
 
 class Workload:
-    """The timed configuration: soccar arenas started from seeded random states (RLGymCPP
-    RandomState distribution), a fresh discrete action per car from the 90-entry table every
-    env step, finished episodes reset to random states."""
+    """One preset: arenas, team sizes, the reset distribution (starts and finished episodes),
+    the action distribution (uniform over the 90-entry table, or biased so that boost and
+    jump are each pressed with probability 0.6)."""
 
     def __init__(self, args):
-        self.num_arenas = args.arenas
-        self.team_size = args.team_size
+        p = PRESETS[args.config]
+        self.preset = args.config
+        self.num_arenas = args.arenas or p["arenas"]
+        self.team_size = args.team_size or p["team"]
+        self.mixed = p["mixed"]
+        self.reset = p["reset"]
+        self.bias = p["bias"]
+        self.graph = p["graph"] and not args.no_graph
+        self.cull = args.cull or p["cull"]
         self.tick_skip = args.tick_skip
-        self.name = args.workload_name
+        self.desc = p["desc"]
+
+    def team_sizes(self):
+        if self.mixed:
+            return np.array([1 + (a % 3) for a in range(self.num_arenas)], np.int32)
+        return None
+
+    def name(self):
+        t = self.tick_skip
+        return (f"{self.desc}, tickSkip {t}: discrete actions -> {t} ticks -> AdvancedObs + masks -> 4 stub rewards + "
+                f"terminals -> {'high-contact' if self.reset == 'high_contact' else 'random-state'} resets")
+
+    def reset_mode(self, rsb):
+        return rsb.RSB_RESET_HIGH_CONTACT if self.reset == "high_contact" else rsb.RSB_RESET_RANDOM_STATE
+
+    def action_weights(self, lut):
+        """Per-action sampling weights: uniform, or boost / jump each with probability 0.6."""
+        if not self.bias:
+            return None
+        b, j = lut["boost"].astype(bool), lut["jump"].astype(bool)
+        w = np.zeros(len(lut))
+        for bb in (False, True):
+            for jj in (False, True):
+                sel = (b == bb) & (j == jj)
+                if sel.any():
+                    w[sel] = (0.6 if bb else 0.4) * (0.6 if jj else 0.4) / sel.sum()
+        return w / w.sum()
 
     def config(self):
-        return {"workload": self.name, "arenas": self.num_arenas, "team_size": self.team_size,
+        ts = "1v1/2v2/3v3 (1:1:1)" if self.mixed else f"{self.team_size}v{self.team_size}"
+        return {"workload": self.name(), "preset": self.preset, "arenas": self.num_arenas, "teams": ts,
                 "tick_skip": self.tick_skip, "narrowphase": "exact-bvh", "state": "fp32",
-                "actions": "uniform over the 90-action table, new each env step",
-                "obs": f"AdvancedObs {51 + 29 * 2 * self.team_size} floats + 90 masks per player",
+                "actions": ("boost and jump each pressed with p=0.6" if self.bias else
+                            "uniform over the 90-action table") + ", new each env step",
+                "obs": "AdvancedObs 51+29*cars floats + 90 masks per player",
                 "rewards": "Goal, TouchBall, VelocityBallToGoal, VelocityPlayerToBall",
-                "terminals": f"goal or {EPISODE_TICKS} ticks; finished arenas reset to random states",
-                "l2": "flushed between timed steps (256 MB write)"}
+                "terminals": f"goal or {EPISODE_TICKS} ticks; finished arenas reset on the device",
+                "graph": self.graph, "l2": "flushed between timed steps (256 MB write)"}
+
+
+class DevArray:
+    """A device pointer of the library seen as a CUDA array (for torch.as_tensor)."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"data": (ptr, False), "shape": shape, "typestr": typestr, "version": 3}
+
+
+def reduce_max(value, dist, device=None):
+    """The largest value over the ranks (timing of the slowest rank)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 # ------------------------------------------------------------------ our arm
@@ -150,23 +216,32 @@ def run_ours(args, rank, world, dist):
     torch.cuda.set_device(dev)
     wl = Workload(args)
     rewards = rsb.default_rewards(pkg.engine_library(), episode_max_ticks=EPISODE_TICKS)
-    batch = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size,
-                      meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank, rewards=rewards,
-                      cull_mode=rsb.RSB_CULL_EXACT)
-    batch.set_action_lut(rsb.default_action_lut(batch.lib))
-    culler = train_culler(batch, rsb, wl, rank) if args.cull == "learned" else None
+    batch = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size or None,
+                      team_sizes=wl.team_sizes(), meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank,
+                      rewards=rewards, cull_mode=rsb.RSB_CULL_EXACT)
+    lut = rsb.default_action_lut(batch.lib)
+    batch.set_action_lut(lut)
+    culler = train_culler(batch, rsb, wl, rank) if wl.cull == "learned" else None
+    reset_mode = wl.reset_mode(rsb)
 
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    gen = torch.Generator(device=f"cuda:{dev}")
     n_cars = max(1, batch.num_cars)
-    actions = torch.empty(n_cars, dtype=torch.int32, device=dev)
+    actions = torch.zeros(n_cars, dtype=torch.int32, device=dev)
+    weights = wl.action_weights(lut)
+    weights_t = torch.tensor(weights, dtype=torch.float32, device=dev) if weights is not None else None
     counter = [0]
+
+    def sample_actions():
+        if weights_t is not None:
+            actions.copy_(torch.multinomial(weights_t, n_cars, replacement=True).to(torch.int32))
+        else:
+            torch.randint(0, rsb.RSB_NUM_ACTIONS, (n_cars,), device=dev, dtype=torch.int32, out=actions)
 
     def one_step(ev=None):
         # the policy's actions arrive on the device; the whole env step stays there
-        actions.random_(0, rsb.RSB_NUM_ACTIONS, generator=gen)
+        sample_actions()
         batch.snapshot(stream=sp)
         batch.set_actions_device(actions.data_ptr(), batch.num_cars, stream=sp)
         if ev is not None:
@@ -177,70 +252,90 @@ def run_ours(args, rank, world, dist):
         batch.build_obs(stream=sp)
         batch.build_rewards_terminals(wl.tick_skip, stream=sp)
         counter[0] += 1
-        batch.reset_done(0x5EED1000 + counter[0], rsb.RSB_RESET_RANDOM_STATE, stream=sp)
+        batch.reset_done(0x5EED1000 + counter[0], reset_mode, stream=sp)
 
     def start(mode):
         # every path starts from the same seeded state and action stream
         batch.set_cull_mode(mode)
-        batch.reset_all(0x5EED0001 + rank, rsb.RSB_RESET_RANDOM_STATE)
-        gen.manual_seed(0x5EED0003 + rank)
+        batch.reset_all(0x5EED0001 + rank, reset_mode)
+        torch.cuda.manual_seed(0x5EED0003 + rank)
         counter[0] = 0
 
-    def timed(clocks_out):
+    def warm():
+        # untimed: settle steps (the per-step cost climbs for a few dozen steps after a
+        # random-state reset while the airborne half of the cars lands), then the warm-up
         with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
+            for _ in range(args.settle + args.warmup):
                 one_step()
         torch.cuda.synchronize()
+
+    def timed(steps, clocks_out, graph=None):
         if dist is not None:
             dist.barrier()
         s0 = batch.stats()
         times, step_times = [], []
         with ClockSampler(dev) as clocks, torch.cuda.stream(stream):
             torch.cuda.synchronize()
-            for _ in range(args.steps):
+            for _ in range(steps):
                 flush.fill_(1.0)  # evict the L2 between timed steps
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 e0.record(stream)
-                one_step(ev)
+                if graph is not None:
+                    graph.replay()
+                else:
+                    one_step(ev)
                 e1.record(stream)
                 e1.synchronize()
                 times.append(e0.elapsed_time(e1))
-                step_times.append(ev[0].elapsed_time(ev[1]))
+                if graph is None:
+                    step_times.append(ev[0].elapsed_time(ev[1]))
             torch.cuda.synchronize()
         clocks_out.append(clocks.summary())
         s1 = batch.stats()
-        total_ms = float(sum(times))
-        if dist is not None:
-            t = torch.tensor([total_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
-            dist.barrier()
-        value = wl.num_arenas * wl.tick_skip * args.steps * world / (total_ms / 1e3)
-        queries = {k: s1[k] - s0[k] for k in ("narrowphase_queries", "culled_queries", "missed_contacts")}
-        return value, total_ms, step_times, queries
+        total_ms = reduce_max(float(sum(times)), dist, dev)
+        value = wl.num_arenas * wl.tick_skip * steps * world / (total_ms / 1e3)
+        delta = {k: s1[k] - s0[k] for k in ("narrowphase_queries", "culled_queries", "missed_contacts", "solver_rows")}
+        return value, total_ms, step_times, delta
 
-    # exact-BVH path (also picks the step kernel's launch configuration)
     clocks = []
+    # exact-BVH path (also picks the step kernel's launch configuration)
     start(rsb.RSB_CULL_EXACT)
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            one_step()
-    torch.cuda.synchronize()
+    warm()
     tune = batch.autotune(wl.tick_skip) if not args.no_autotune else []
+    extra = {}
+    steps = args.steps
+    if wl.preset == "c4":
+        steps = max(steps, 4096 // wl.tick_skip)  # one 4096-tick rollout
     start(rsb.RSB_CULL_EXACT)
-    ex_value, ex_ms, ex_steps, ex_q = timed(clocks)
-    value, total_ms, step_times, queries = ex_value, ex_ms, ex_steps, ex_q
+    warm()
+    if wl.graph:
+        # kernel time from a short eager segment, then the env step captured once and replayed
+        _, _, kernel_steps, _ = timed(3, [])
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            with torch.cuda.graph(graph, stream=stream):
+                one_step()
+        torch.cuda.synchronize()
+        value, total_ms, _, queries = timed(steps, clocks, graph)
+        step_times = kernel_steps
+        extra["graph"] = {"launches_per_replay": 6, "note": "reset seeds are fixed inside the captured step"}
+        ex_value = value
+        del graph
+    else:
+        value, total_ms, step_times, queries = timed(steps, clocks)
+        ex_value, ex_ms, ex_steps, ex_q = value, total_ms, step_times, queries
     learned = None
     if culler is not None:
         start(rsb.RSB_CULL_LEARNED)
-        value, total_ms, step_times, queries = timed(clocks)
+        warm()
+        value, total_ms, step_times, queries = timed(steps, clocks)
         # the same run once more with the skipped tests executed and checked
         start(rsb.RSB_CULL_LEARNED_AUDIT)
         s0 = batch.stats()
         with torch.cuda.stream(stream):
-            for _ in range(args.warmup + args.steps):
+            for _ in range(args.settle + args.warmup + min(steps, 64)):
                 one_step()
         torch.cuda.synchronize()
         s1 = batch.stats()
@@ -248,10 +343,13 @@ def run_ours(args, rank, world, dist):
         learned = {"train": culler, "culled_fraction": queries["culled_queries"] / max(1, tested),
                    "static_tests": queries, "audit_missed_contacts": s1["missed_contacts"] - s0["missed_contacts"],
                    "audit_arenas_reverted": s1["arenas_reverted"],
-                   "exact_bvh": {"value": ex_value, "ms_per_step": ex_ms / args.steps,
+                   "exact_bvh": {"value": ex_value, "ms_per_step": ex_ms / steps,
                                  "kernel_ms": statistics.mean(ex_steps), "static_tests": ex_q},
                    "learned_over_exact": value / ex_value}
         batch.set_cull_mode(rsb.RSB_CULL_LEARNED)
+    if wl.preset == "c4":
+        extra["stress"] = stress_events(pkg, batch, wl, rank, dev)
+        extra["stress"]["solver_rows_per_arena_tick"] = queries["solver_rows"] / (wl.num_arenas * wl.tick_skip * steps)
 
     # e2e through the public API with host buffers, as the collector's host path runs it:
     # host actions in (H2D), step, obs / masks / rewards / terminals back to the host (D2H),
@@ -269,11 +367,11 @@ def run_ours(args, rank, world, dist):
         obs, masks, rew, term = batch.copy_obs(), batch.copy_masks(), batch.copy_rewards(), batch.copy_terminals()
         done = np.nonzero(term)[0].astype(np.int32)
         if done.size:
-            batch.reset_arenas(done, 0x5EED2000 + k, rsb.RSB_RESET_RANDOM_STATE)
+            batch.reset_arenas(done, 0x5EED2000 + k, reset_mode)
         e2e_times.append(time.perf_counter() - t0)
         h2d.append(4 * batch.num_cars + 4 * done.size)
         d2h.append(obs.nbytes + masks.nbytes + rew.nbytes + term.nbytes)
-    e2e_value = wl.num_arenas * wl.tick_skip * world / statistics.median(e2e_times)
+    e2e_value = wl.num_arenas * wl.tick_skip * world / reduce_max(statistics.median(e2e_times), dist, dev)
 
     # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
     # state read + written per launch (the library reports it), over the kernel's own time
@@ -285,24 +383,68 @@ def run_ours(args, rank, world, dist):
     if learned is not None:
         cfg["narrowphase"] = "learned cull (exact BVH for every body the bound does not clear)"
     res = {
-        "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random states)",
         "config": cfg,
         "roofline": {"bound": "hbm", "kernel": "stepKernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                      "bytes_per_launch": alg_bytes, "kernel_ms": kernel_s * 1e3,
-                     "kernel_share": statistics.mean(step_times) / (total_ms / args.steps)},
+                     "kernel_share": statistics.mean(step_times) / (total_ms / steps)},
         "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": int(statistics.mean(h2d)),
                 "d2h_bytes_per_step": int(statistics.mean(d2h))},
         # per env step: action expansion, (culler,) step, obs + masks, rewards + terminals, reset
-        "gpu_launches": args.steps * (6 if learned is not None else 5),
+        "gpu_launches": steps * (6 if learned is not None else 5),
         "learned_cull": learned,
         "autotune": tune,
         "clocks": clocks[-1],
         "clocks_exact": clocks[0],
-    }
+    } | extra
     return res
+
+
+def stress_events(pkg, trained, wl, rank, dev):
+    """Goal and demo events of 64 env steps on the exact and on the learned path, run in
+    lockstep on two fresh batches built the same way (same seeds, same actions), step by
+    step (goals: terminal flag 1; demoed cars: the demo flag of the obs rows)."""
+    import torch
+    rsb = pkg.rsb
+    weights, margin = trained.culler_get()
+    lut = rsb.default_action_lut(trained.lib)
+    w = wl.action_weights(lut)
+    mk = []
+    for mode in (rsb.RSB_CULL_EXACT, rsb.RSB_CULL_LEARNED):
+        b = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size or None,
+                      team_sizes=wl.team_sizes(), meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank,
+                      rewards=rsb.default_rewards(pkg.engine_library(), episode_max_ticks=EPISODE_TICKS),
+                      cull_mode=mode)
+        b.set_action_lut(lut)
+        if mode != rsb.RSB_CULL_EXACT:
+            b.culler_set(weights, margin)
+        b.reset_all(0x5EED0001 + rank, wl.reset_mode(rsb))
+        obs = torch.as_tensor(DevArray(b.device_ptr(rsb.RSB_BUF_OBS), (b.num_cars, b.obs_stride), "<f4"), device=dev)
+        term = torch.as_tensor(DevArray(b.device_ptr(rsb.RSB_BUF_TERMINALS), (wl.num_arenas,), "|u1"), device=dev)
+        mk.append((b, obs, term))
+    rng = np.random.default_rng(0x5EED0006 + rank)
+    seqs = [[], []]
+    for step in range(64):
+        idx = rng.choice(len(lut), mk[0][0].num_cars, p=w).astype(np.int32)
+        for k, (b, obs, term) in enumerate(mk):
+            b.set_actions(idx)
+            b.step(wl.tick_skip)
+            b.build_obs()
+            b.build_rewards_terminals(wl.tick_skip)
+            b.sync()
+            seqs[k].append((int((term == 1).sum().item()), int((obs[:, 51 + 27] > 0.5).sum().item())))
+            b.reset_done(0x5EED4000 + step, wl.reset_mode(rsb))
+    same_state = (mk[0][0].get_cars().tobytes() == mk[1][0].get_cars().tobytes() and
+                  mk[0][0].get_balls().tobytes() == mk[1][0].get_balls().tobytes())
+    learned_stats = mk[1][0].stats()
+    ex, le = seqs
+    return {"steps_compared": len(ex), "goals_exact": sum(g for g, _ in ex), "goals_learned": sum(g for g, _ in le),
+            "demoed_car_steps_exact": sum(d for _, d in ex), "demoed_car_steps_learned": sum(d for _, d in le),
+            "event_agreement": sum(a == b for a, b in zip(ex, le)) / len(ex), "final_state_identical": same_state,
+            "culled_queries": learned_stats["culled_queries"]}
 
 
 # ------------------------------------------------------------------ CPU reference
@@ -310,19 +452,24 @@ def run_ours(args, rank, world, dist):
 def cpu_reference(args, sample_s=10.0, threads=None):
     """The reference's CPU path for the same env step: RocketSim arenas stepped on all host
     threads, then RLGymCPP's GameState / AdvancedObs / DefaultAction masks / stub rewards /
-    terminal conditions, then the finished arenas reset to random states."""
+    terminal conditions, then the finished arenas reset.  (The CPU reference has no
+    high-contact start; that preset's CPU sample starts from random states.)"""
     pkg = load_pkg()
     rsb = pkg.rsb
     lib = rsb.load_library(ORACLE_LIB)
     threads = threads or os.cpu_count() or 1
-    n = min(args.arenas, 64 * threads)
     wl = Workload(args)
-    b = rsb.Batch(lib, n, team_size=wl.team_size, meshes_path=pkg.MESHES_DIR, threads=threads,
+    n = min(wl.num_arenas, 64 * threads)
+    ts = wl.team_sizes()
+    b = rsb.Batch(lib, n, team_size=wl.team_size or None, team_sizes=None if ts is None else ts[:n],
+                  meshes_path=pkg.MESHES_DIR, threads=threads,
                   rewards=rsb.default_rewards(lib, episode_max_ticks=EPISODE_TICKS))
     b.reset_all(0x5EED0001, rsb.RSB_RESET_RANDOM_STATE)
-    b.set_action_lut(rsb.default_action_lut(lib))
+    lut = rsb.default_action_lut(lib)
+    b.set_action_lut(lut)
     rng = np.random.default_rng(0x5EED0003)
-    pool = [rng.integers(0, rsb.RSB_NUM_ACTIONS, max(1, b.num_cars)).astype(np.int32) for _ in range(16)]
+    w = wl.action_weights(lut)
+    pool = [rng.choice(len(lut), max(1, b.num_cars), p=w).astype(np.int32) for _ in range(16)]
 
     def env_step(k):
         b.set_actions(pool[k % 16][:b.num_cars])
@@ -358,21 +505,18 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--arenas", type=int, default=65536)
-    ap.add_argument("--team-size", type=int, default=3)
+    ap.add_argument("--config", default="c3", choices=sorted(PRESETS))
+    ap.add_argument("--arenas", type=int, default=None)
+    ap.add_argument("--team-size", type=int, default=None)
     ap.add_argument("--tick-skip", type=int, default=8)
-    ap.add_argument("--workload-name", default=None)
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--cull", default="learned", choices=["learned", "exact"])
+    ap.add_argument("--settle", type=int, default=40, help="untimed steps after each reset before warm-up")
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--cull", default=None, choices=["learned", "exact"])
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    if args.workload_name is None:
-        t = args.team_size
-        args.workload_name = (f"soccar {t}v{t} x {args.arenas} arenas, tickSkip {args.tick_skip}: random discrete "
-                              f"actions -> {args.tick_skip} ticks -> AdvancedObs + masks -> 4 stub rewards + "
-                              "terminals -> random-state resets")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -26,7 +26,7 @@ struct EngineView {
     uint32_t seed;
     const uint32_t* cull;          // per-arena body bits from the learned culler, or null
     int32_t cullAudit;             // run culled static tests anyway and count what they find
-    unsigned long long* counters;  // [static tests run, tests culled, culled tests that hit], or null
+    unsigned long long* counters;  // [static tests run, tests culled, culled tests that hit, solver rows], or null
 };
 
 RSB_HD void initBodyCommon(Body& b) {
@@ -226,12 +226,14 @@ RSB_HD void stepArena(const EngineView& D, int a, int ticks, ArenaSim& A) {
     W.cullAudit = D.cullAudit;
     W.nStatic = W.nCulled = W.nMissed = 0;
     W.cullMissed = 0;
+    W.nRows = 0;
     for (int t = 0; t < ticks; t++) arenaTick(A);
 #if defined(__CUDA_ARCH__)
     if (D.counters) {
         atomicAdd(&D.counters[0], (unsigned long long)W.nStatic);
         atomicAdd(&D.counters[1], (unsigned long long)W.nCulled);
         if (W.nMissed) atomicAdd(&D.counters[2], (unsigned long long)W.nMissed);
+        atomicAdd(&D.counters[3], (unsigned long long)W.nRows);
     }
 #endif
     storeBall(D, a, W.b[0]);

@@ -61,6 +61,7 @@ struct World {
     int32_t cullAudit;
     mutable uint32_t nStatic, nCulled, nMissed;  // static tests run / skipped / skipped but hit
     mutable uint32_t cullMissed;                 // WS_CULL_MISS once a skipped test would have hit
+    mutable uint32_t nRows;                      // solver rows (contact + friction) set up this launch
     RegOrder reg;
 };
 
@@ -1074,6 +1075,7 @@ RSB_HD void solveIslands(World& W) {
         b.spFric = b.spRest = b.spDist = 0.f;
         b.spNormal = v3zero();
     }
+    W.nRows += (uint32_t)(Sv.nc + Sv.nf);
     solverIterate(Sv);
     solverWriteBack(Sv, W.b, W.noRot, dt);
 }

@@ -714,6 +714,7 @@ rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out) {
     out->narrowphase_queries = c[0];
     out->culled_queries = c[1];
     out->missed_contacts = c[2];
+    out->solver_rows = c[3];
     uint64_t reverted = 0, bits = 0;
     for (uint32_t v : status) {
         bits |= v;

@@ -571,6 +571,30 @@ RSB_HD void releaseManifold(World& W, int idx) {
 
 RSB_HD float sq(float x) { return x * x; }
 
+// True when some separating axis (the triangle normal, the box axes, or a box axis crossed
+// with a triangle edge) puts the triangle more than `limit` away from the box of implicit
+// half extents `he` at `x`.  The gap along an axis bounds the distance between the two
+// from below, so GJK could not report a contact for such a triangle.
+RSB_HD bool boxTriFar(const Xf& x, V3 he, const V3* v, float limit) {
+    const V3 a0 = x.b.col(0), a1 = x.b.col(1), a2 = x.b.col(2);
+    const V3 p0 = v[0] - x.o, p1 = v[1] - x.o, p2 = v[2] - x.o;
+    auto sep = [&](V3 L) -> bool {
+        const float l2 = dot(L, L);
+        if (l2 < 1e-12f) return false;
+        const float r = fabsf(dot(a0, L)) * he.x + fabsf(dot(a1, L)) * he.y + fabsf(dot(a2, L)) * he.z;
+        const float t0 = dot(p0, L), t1 = dot(p1, L), t2 = dot(p2, L);
+        const float gap = fmaxf(fmin_(t0, fmin_(t1, t2)) - r, -r - fmax_(t0, fmax_(t1, t2)));
+        return gap > limit * sqrtf(l2);
+    };
+    const V3 e0 = p1 - p0, e1 = p2 - p1, e2 = p0 - p2;
+    if (sep(cross(e0, e1)) || sep(a0) || sep(a1) || sep(a2)) return true;
+    const V3 ax[3] = {a0, a1, a2}, ed[3] = {e0, e1, e2};
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            if (sep(cross(ax[i], ed[j]))) return true;
+    return false;
+}
+
 // Car box vs one arena mesh: the compound's child algorithm is btConvexConcaveCollisionAlgorithm
 // (btConvexConcaveCollisionAlgorithm.cpp:60-250), each overlapping triangle through
 // btConvexConvexAlgorithm's GJK (btConvexConvexAlgorithm.cpp:268-590).
@@ -599,6 +623,8 @@ RSB_HD void collideBoxMesh(World& W, int mesh, int ci, const Xf& childXf, Manifo
             if (dist > man.cbt + 0.f) return true;
             tn *= -1.f;
         }
+        // separated well beyond the contact distance: GJK would find no contact
+        if (boxTriFar(childXf, box.he, v, (C.boxMargin + 0.f) + man.cbt + 0.02f)) return true;
         ConvexShape triS = makeTri(v, 0.f);
         GjkOut g = gjkPairDetector(W.epa, box, childXf, triS, xfIdentity(), maxDist2);
         if (g.overflow) W.status |= WS_EPA_OVERFLOW;

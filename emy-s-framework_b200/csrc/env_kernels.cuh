@@ -173,7 +173,11 @@ RSB_D float obsValue(const ObsShared& S, int la, int p, int col) {
     return obsCarValue(S, la, q, orange, j);
 }
 
-__global__ void __launch_bounds__(32) obsKernel(EnvView E, EnvTables Tb) {
+// A block stages the inputs of 32 arenas (one arena per thread of its first warp), then
+// all of its warps build and write the arenas' rows: the rows of consecutive arenas are
+// contiguous, so the writes are coalesced.
+constexpr int OBS_THREADS = 256;
+__global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb) {
     __shared__ ObsShared S;
     const int lane = threadIdx.x;
     const int a0 = blockIdx.x * OBS_ARENAS;
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(32) obsKernel(EnvView E, EnvTables Tb) {
     const int aEnd = min(a0 + OBS_ARENAS, E.N);
     const int a = a0 + lane;
     const int row0 = E.carOffset[a0];
-    if (a < aEnd) {
+    if (lane < OBS_ARENAS && a < aEnd) {
         const int T = E.teamSize[a], M = 2 * T;
         S.in[OI_TEAM][lane] = (float)T;
         for (int k = 0; k < 3; k++) {
@@ -248,12 +252,12 @@ __global__ void __launch_bounds__(32) obsKernel(EnvView E, EnvTables Tb) {
             S.in[OI_PAD + NUM_PADS + i][lane] = active(m) ? 1.f : 1.f / (1.f + cool[d]);
         }
     }
-    __syncwarp();
+    __syncthreads();
     const int rows = E.carOffset[aEnd] - row0;
     const int stride = E.stride;
     float* out = E.obs + (size_t)row0 * stride;
     const int n = rows * stride;
-    for (int e = lane; e < n; e += 32) {
+    for (int e = lane; e < n; e += OBS_THREADS) {
         const int r = e / stride, col = e - r * stride;
         const uint16_t ro = S.rowOf[r];
         out[e] = obsValue(S, ro & 0xff, ro >> 8, col);
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(32) obsKernel(EnvView E, EnvTables Tb) {
     // masks: rows * 90 bytes, 4-byte aligned (every arena has an even number of cars)
     uint32_t* mout = reinterpret_cast<uint32_t*>(E.masks + (size_t)row0 * RSB_NUM_ACTIONS);
     const int nw = rows * RSB_NUM_ACTIONS / 4;
-    for (int w = lane; w < nw; w += 32) {
+    for (int w = lane; w < nw; w += OBS_THREADS) {
         uint32_t word = 0;
         for (int t = 0; t < 4; t++) {
             const int e = 4 * w + t, r = e / RSB_NUM_ACTIONS, i = e - r * RSB_NUM_ACTIONS;

@@ -121,7 +121,7 @@ struct rsb_handle {
     int numTris = 0;
     std::shared_ptr<ArenaStaticHost> host;
     // launch configuration of the step kernel (indices into kStepVariants / kStepBlocks)
-    int stepVariant = 0, stepBlock = 2;
+    int stepVariant = 0, stepBlock = 1;
     uint32_t* dScratch = nullptr;   // the autotuner's copy of the arena records
     EnvTables tables{};
     bool hasRewards = false;
@@ -1115,7 +1115,7 @@ rsb_status rsb_snapshot(rsb_handle* h, void*) { return h ? RSB_OK : RSB_ERR_INVA
 rsb_status rsb_build_obs(rsb_handle* h, void* stream) {
     if (!h) return RSB_ERR_INVALID;
     RSB_CUDA(cudaSetDevice(h->device));
-    obsKernel<<<(h->N + OBS_ARENAS - 1) / OBS_ARENAS, 32, 0, pick(h, stream)>>>(envView(h), h->tables);
+    obsKernel<<<(h->N + OBS_ARENAS - 1) / OBS_ARENAS, OBS_THREADS, 0, pick(h, stream)>>>(envView(h), h->tables);
     RSB_CUDA(cudaGetLastError());
     return RSB_OK;
 }

@@ -443,7 +443,7 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
     S.triInfo = out.triInfo.data();
     S.bpCells = out.bpCells.data();
 
-    // ---- mesh occupancy grid (see ArenaStatic::occ): 64 uu voxels over the arena
+    // ---- mesh occupancy grid (see ArenaStatic::occ): 64 uu voxels over the arena, a mesh bit each
     {
         const float cell = 64.f * kUuToBt, tol = 2.f * kUuToBt;
         const V3 gmn = V3{-4400.f, -6300.f, -200.f} * kUuToBt, gmx = V3{4400.f, 6300.f, 2300.f} * kUuToBt;
@@ -453,9 +453,12 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
         S.occY = (int)std::ceil((gmx.y - gmn.y) / cell);
         S.occZ = (int)std::ceil((gmx.z - gmn.z) / cell);
         const size_t nv = (size_t)S.occX * S.occY * S.occZ;
-        out.occ.assign((nv + 31) / 32, 0u);
+        out.occ.assign(nv, 0);
         const float halfDiag = 0.5f * cell * std::sqrt(3.f);
         const size_t ntri = out.triVerts.size() / 3;
+        std::vector<int> meshOf(ntri, 0);
+        for (int m = 0; m < S.numMeshes; m++)
+            for (int t = 0; t < S.meshes[m].triCount; t++) meshOf[S.meshes[m].triOff + t] = m;
         for (size_t t = 0; t < ntri; t++) {
             const V3 a = out.triVerts[3 * t], b = out.triVerts[3 * t + 1], c = out.triVerts[3 * t + 2];
             const V3 mn = vmin(vmin(a, b), c) - V3{tol, tol, tol}, mx = vmax(vmax(a, b), c) + V3{tol, tol, tol};
@@ -474,7 +477,7 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
                         // the triangle's plane must come within the voxel's half diagonal
                         if (flat && std::fabs(dot(n, centre - a)) > halfDiag + tol) continue;
                         const size_t v = ((size_t)x * S.occY + y) * S.occZ + z;
-                        out.occ[v >> 5] |= 1u << (v & 31);
+                        out.occ[v] |= (uint16_t)(1u << meshOf[t]);
                     }
         }
         S.occ = out.occ.data();
@@ -484,7 +487,7 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
 
 ArenaStatic deviceView(const ArenaStaticHost& h, const BvhNode* nodes, const BvhSubtree* subs,
                        const V3* triVerts, const TriEdgeInfo* triInfo, const uint32_t* bpCells,
-                       const uint32_t* occ) {
+                       const uint16_t* occ) {
     ArenaStatic v = h.view;
     v.occ = occ;
     v.nodes = nodes;

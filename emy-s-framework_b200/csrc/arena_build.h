@@ -13,7 +13,7 @@ struct ArenaStaticHost {
     std::vector<V3> triVerts;
     std::vector<TriEdgeInfo> triInfo;
     std::vector<uint32_t> bpCells;
-    std::vector<uint32_t> occ;
+    std::vector<uint16_t> occ;
     ArenaStatic view;  // pointers into the vectors above (host addresses)
     std::string error;
 };
@@ -26,6 +26,6 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out);
 // Re-points out.view at a device copy whose buffers are given.
 ArenaStatic deviceView(const ArenaStaticHost& h, const BvhNode* nodes, const BvhSubtree* subs,
                        const V3* triVerts, const TriEdgeInfo* triInfo, const uint32_t* bpCells,
-                       const uint32_t* occ);
+                       const uint16_t* occ);
 
 }  // namespace rsb

@@ -67,11 +67,12 @@ struct ArenaStatic {
     const V3* triVerts;        // 3 per triangle, Bullet units
     const TriEdgeInfo* triInfo;
     const uint32_t* bpCells;   // bit s set: static object s registered in the cell
-    // Mesh occupancy grid (Bullet units): bit v set when some mesh triangle may pass
-    // through voxel v (the triangle's AABB overlaps the voxel and its plane crosses it,
-    // both tested with a tolerance).  A region whose voxels are all clear holds no
-    // triangle, so mesh queries confined to it cannot find anything and are skipped.
-    const uint32_t* occ;
+    // Mesh occupancy grid (Bullet units): bit m of voxel v set when some triangle of mesh
+    // m may pass through the voxel (the triangle's AABB overlaps the voxel and its plane
+    // crosses it, both tested with a tolerance).  A mesh with no bit in the voxels of a
+    // region holds no triangle there, so its queries confined to the region cannot find
+    // anything and are skipped.
+    const uint16_t* occ;
     V3 occMin;
     float occInvCell;
     int occX, occY, occZ;
@@ -85,21 +86,19 @@ struct ArenaStatic {
     V3 planeShapeMin[NUM_PLANES], planeShapeMax[NUM_PLANES];  // btStaticPlaneShape::getAabb
 };
 
-// True when any voxel overlapped by the box [mn, mx] may hold a mesh triangle (boxes
-// reaching outside the grid count as occupied).
-RSB_HD bool occAny(const ArenaStatic& S, V3 mn, V3 mx) {
+// The meshes that may have a triangle in a voxel overlapped by the box [mn, mx] (boxes
+// reaching outside the grid get every mesh).
+RSB_HD uint32_t occMask(const ArenaStatic& S, V3 mn, V3 mx) {
     const float f = S.occInvCell;
     int x0 = (int)floorf((mn.x - S.occMin.x) * f), x1 = (int)floorf((mx.x - S.occMin.x) * f);
     int y0 = (int)floorf((mn.y - S.occMin.y) * f), y1 = (int)floorf((mx.y - S.occMin.y) * f);
     int z0 = (int)floorf((mn.z - S.occMin.z) * f), z1 = (int)floorf((mx.z - S.occMin.z) * f);
-    if (!(x0 >= 0 && y0 >= 0 && z0 >= 0 && x1 < S.occX && y1 < S.occY && z1 < S.occZ)) return true;
+    if (!(x0 >= 0 && y0 >= 0 && z0 >= 0 && x1 < S.occX && y1 < S.occY && z1 < S.occZ)) return 0xffffffffu;
+    uint32_t m = 0;
     for (int x = x0; x <= x1; x++)
         for (int y = y0; y <= y1; y++)
-            for (int z = z0; z <= z1; z++) {
-                const int v = (x * S.occY + y) * S.occZ + z;
-                if ((S.occ[v >> 5] >> (v & 31)) & 1u) return true;
-            }
-    return false;
+            for (int z = z0; z <= z1; z++) m |= S.occ[(x * S.occY + y) * S.occZ + z];
+    return m;
 }
 
 // ------------------------------------------------------------ BVH queries (device)

@@ -395,8 +395,8 @@ RSB_HD void collideBallMesh(World& W, int mesh, Manifold& man) {
     V3 amn, amx;
     ballAabb(P, ball.xf, amn, amx);  // convexInTriangleSpace == ball transform (mesh at identity)
     M3 invB = inverse(ball.xf.b);
-    // no triangle near the query box: the walk below could not report one
-    if (occAny(*W.S, amn - V3{kOccTol, kOccTol, kOccTol}, amx + V3{kOccTol, kOccTol, kOccTol}))
+    // no triangle of this mesh near the query box: the walk below could not report one
+    if ((occMask(*W.S, amn - V3{kOccTol, kOccTol, kOccTol}, amx + V3{kOccTol, kOccTol, kOccTol}) >> mesh) & 1u)
     bvhQueryAabb(*W.S, mesh, amn, amx, [&](int tri) {
         V3 v[3];
         triVerts(*W.S, mesh, tri, v);
@@ -610,7 +610,7 @@ RSB_HD void collideBoxMesh(World& W, int mesh, int ci, const Xf& childXf, Manifo
     bool responds = carResponds(W, ci);
     bool found = false;
     if (!cullSkip(W, 1 + ci) &&
-        occAny(*W.S, amn - V3{kOccTol, kOccTol, kOccTol}, amx + V3{kOccTol, kOccTol, kOccTol})) {
+        ((occMask(*W.S, amn - V3{kOccTol, kOccTol, kOccTol}, amx + V3{kOccTol, kOccTol, kOccTol}) >> mesh) & 1u)) {
     bvhQueryAabb(*W.S, mesh, amn, amx, [&](int tri) {
         V3 v[3];
         triVerts(*W.S, mesh, tri, v);
@@ -811,13 +811,13 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
     hit.obj = -1;
     hit.normal = v3zero();
     const int rayBody = ignoreObj - OBJ_BALL;  // the casting car's body
-    // no mesh triangle near the segment: no mesh can be hit
+    // meshes with a triangle near the segment: no other mesh can be hit
     const V3 tolv{kOccTol, kOccTol, kOccTol};
-    const bool meshNear = occAny(S, vmin(from, to) - tolv, vmax(from, to) + tolv);
+    const uint32_t meshNear = occMask(S, vmin(from, to) - tolv, vmax(from, to) + tolv);
     auto testObj = [&](int o) {
         if (hit.fraction == 0.f) return;
         if (o == ignoreObj) return;
-        if (o < MAX_MESHES && !meshNear) return;
+        if (o < MAX_MESHES && !((meshNear >> o) & 1u)) return;
         if (o < NUM_STATICS) {
             if (cullSkip(W, rayBody)) return;
             if ((W.cull >> rayBody) & 1u) {

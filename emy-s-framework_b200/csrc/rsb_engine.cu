@@ -43,7 +43,7 @@ struct DevStatic {
     V3* triVerts = nullptr;
     TriEdgeInfo* triInfo = nullptr;
     uint32_t* bpCells = nullptr;
-    uint32_t* occ = nullptr;
+    uint16_t* occ = nullptr;
     ArenaStatic view{};
 };
 

@@ -15,6 +15,7 @@
 #include "arena_build.h"
 #include "phys/consts.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -459,6 +460,20 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
         std::vector<int> meshOf(ntri, 0);
         for (int m = 0; m < S.numMeshes; m++)
             for (int t = 0; t < S.meshes[m].triCount; t++) meshOf[S.meshes[m].triOff + t] = m;
+        // the BVH leaf (node index within its mesh) of every triangle; the voxel keys hold
+        // 12 bits of leaf index and 10 bits of triangle index
+        for (int m = 0; m < S.numMeshes; m++)
+            if (S.meshes[m].nodeCount > 4096 || S.meshes[m].triCount > 1024) {
+                out.error = "mesh too large for the voxel triangle lists";
+                return false;
+            }
+        std::vector<int> leafOf(ntri, -1);
+        for (int m = 0; m < S.numMeshes; m++)
+            for (int k = 0; k < S.meshes[m].nodeCount; k++) {
+                const BvhNode& nd = out.nodes[(size_t)S.meshes[m].nodeOff + k];
+                if (nd.data >= 0) leafOf[(size_t)S.meshes[m].triOff + nd.data] = k;
+            }
+        std::vector<std::pair<uint32_t, uint32_t>> lists;  // (voxel, key)
         for (size_t t = 0; t < ntri; t++) {
             const V3 a = out.triVerts[3 * t], b = out.triVerts[3 * t + 1], c = out.triVerts[3 * t + 2];
             const V3 mn = vmin(vmin(a, b), c) - V3{tol, tol, tol}, mx = vmax(vmax(a, b), c) + V3{tol, tol, tol};
@@ -478,18 +493,34 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
                         if (flat && std::fabs(dot(n, centre - a)) > halfDiag + tol) continue;
                         const size_t v = ((size_t)x * S.occY + y) * S.occZ + z;
                         out.occ[v] |= (uint16_t)(1u << meshOf[t]);
+                        const int m = meshOf[t], lt = (int)t - S.meshes[m].triOff;
+                        lists.emplace_back((uint32_t)v, voxKey(m, leafOf[t], lt));
                     }
         }
         S.occ = out.occ.data();
+        // per-voxel triangle lists, each sorted by (mesh, BVH leaf): the order in which the
+        // meshes' BVH walks would report them
+        std::sort(lists.begin(), lists.end());
+        out.voxOff.assign(nv + 1, 0u);
+        out.voxList.resize(lists.size());
+        for (size_t i = 0; i < lists.size(); i++) {
+            out.voxOff[lists[i].first + 1]++;
+            out.voxList[i] = lists[i].second;
+        }
+        for (size_t v = 0; v < nv; v++) out.voxOff[v + 1] += out.voxOff[v];
+        S.voxOff = out.voxOff.data();
+        S.voxList = out.voxList.data();
     }
     return true;
 }
 
 ArenaStatic deviceView(const ArenaStaticHost& h, const BvhNode* nodes, const BvhSubtree* subs,
                        const V3* triVerts, const TriEdgeInfo* triInfo, const uint32_t* bpCells,
-                       const uint16_t* occ) {
+                       const uint16_t* occ, const uint32_t* voxOff, const uint32_t* voxList) {
     ArenaStatic v = h.view;
     v.occ = occ;
+    v.voxOff = voxOff;
+    v.voxList = voxList;
     v.nodes = nodes;
     v.subs = subs;
     v.triVerts = triVerts;

@@ -73,6 +73,11 @@ struct ArenaStatic {
     // region holds no triangle there, so its queries confined to the region cannot find
     // anything and are skipped.
     const uint16_t* occ;
+    // Per voxel (CSR: voxOff[v] .. voxOff[v + 1] into voxList), the mesh triangles marked in
+    // it as voxKey(mesh, BVH leaf node, triangle), sorted: the order the meshes' BVH walks
+    // visit them.
+    const uint32_t* voxOff;
+    const uint32_t* voxList;
     V3 occMin;
     float occInvCell;
     int occX, occY, occZ;
@@ -85,6 +90,10 @@ struct ArenaStatic {
     V3 planeBpMin[NUM_PLANES], planeBpMax[NUM_PLANES];
     V3 planeShapeMin[NUM_PLANES], planeShapeMax[NUM_PLANES];  // btStaticPlaneShape::getAabb
 };
+
+RSB_HD uint32_t voxKey(int mesh, int leaf, int tri) {
+    return ((uint32_t)mesh << 22) | ((uint32_t)leaf << 10) | (uint32_t)tri;
+}
 
 // The meshes that may have a triangle in a voxel overlapped by the box [mn, mx] (boxes
 // reaching outside the grid get every mesh).

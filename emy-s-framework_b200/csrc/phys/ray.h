@@ -58,6 +58,76 @@ RSB_HD void rayVsMesh(const ArenaStatic& S, int mesh, V3 from, V3 to, RayHit& hi
     });
 }
 
+// The closest hit over the meshes in `meshes` (bit m = mesh m), exactly as rayVsMesh called
+// for those meshes in ascending order would report it, found from the voxel triangle lists
+// instead of the BVH walks: the lists of the voxels around the segment hold every triangle
+// the segment can touch, a triangle is tested only if its BVH leaf passes the two tests the
+// walk applies to it (a leaf that passes them has ancestors that pass them), and the
+// candidates are taken in (mesh, leaf) order, the order of the walks.  Returns false, with
+// `hit` untouched, when the segment leaves the grid or has more candidates than fit.
+constexpr int kRayCandidates = 48;
+RSB_HD bool rayVsMeshesVox(const ArenaStatic& S, uint32_t meshes, V3 src, V3 dst, float tol, RayHit& hit) {
+    const V3 mn = vmin(src, dst) - V3{tol, tol, tol}, mx = vmax(src, dst) + V3{tol, tol, tol};
+    const float f = S.occInvCell;
+    const int x0 = (int)floorf((mn.x - S.occMin.x) * f), x1 = (int)floorf((mx.x - S.occMin.x) * f);
+    const int y0 = (int)floorf((mn.y - S.occMin.y) * f), y1 = (int)floorf((mx.y - S.occMin.y) * f);
+    const int z0 = (int)floorf((mn.z - S.occMin.z) * f), z1 = (int)floorf((mx.z - S.occMin.z) * f);
+    if (!(x0 >= 0 && y0 >= 0 && z0 >= 0 && x1 < S.occX && y1 < S.occY && z1 < S.occZ)) return false;
+    uint32_t cand[kRayCandidates];
+    int nc = 0;
+    for (int x = x0; x <= x1; x++)
+        for (int y = y0; y <= y1; y++)
+            for (int z = z0; z <= z1; z++) {
+                const int v = (x * S.occY + y) * S.occZ + z;
+                for (uint32_t i = S.voxOff[v], e = S.voxOff[v + 1]; i < e; i++) {
+                    const uint32_t key = S.voxList[i];
+                    if (!((meshes >> (key >> 22)) & 1u)) continue;
+                    // sorted insert without duplicates
+                    int p = nc;
+                    while (p > 0 && cand[p - 1] > key) p--;
+                    if (p > 0 && cand[p - 1] == key) continue;
+                    if (nc == kRayCandidates) return false;
+                    for (int q = nc; q > p; q--) cand[q] = cand[q - 1];
+                    cand[p] = key;
+                    nc++;
+                }
+            }
+    // the ray set-up of bvhQueryRay
+    const V3 rayDir = safeNormalized(dst - src);
+    const float lambdaMax = dot(rayDir, dst - src);
+    V3 inv;
+    inv.x = rayDir.x == 0.f ? kLargeFloat : 1.f / rayDir.x;
+    inv.y = rayDir.y == 0.f ? kLargeFloat : 1.f / rayDir.y;
+    inv.z = rayDir.z == 0.f ? kLargeFloat : 1.f / rayDir.z;
+    const unsigned sign[3] = {inv.x < 0.f, inv.y < 0.f, inv.z < 0.f};
+    const V3 rmn = vmin(src, dst), rmx = vmax(src, dst);
+    int cur = -1;
+    uint16_t qmn[3], qmx[3];
+    float cbf = hit.fraction;
+    for (int c = 0; c < nc; c++) {
+        const int m = (int)(cand[c] >> 22), leaf = (int)((cand[c] >> 10) & 0xFFFu), tri = (int)(cand[c] & 0x3FFu);
+        const MeshDesc& md = S.meshes[m];
+        if (m != cur) {
+            if (hit.fraction == 0.f) break;  // castRay tests no further object after an exact hit
+            cur = m;
+            bvhQuantizeClamp(md, rmn, 0, qmn);
+            bvhQuantizeClamp(md, rmx, 1, qmx);
+            cbf = hit.fraction;
+        }
+        const BvhNode& nd = S.nodes[md.nodeOff + leaf];
+        if (!qOverlap(qmn, qmx, nd.qmin, nd.qmax)) continue;
+        V3 bounds[2];
+        bounds[0] = bvhUnquantize(md, nd.qmin);
+        bounds[1] = bvhUnquantize(md, nd.qmax);
+        float param = 1.f;
+        if (!rayAabb2(src, inv, sign, bounds, param, 0.f, lambdaMax)) continue;
+        V3 v[3];
+        triVerts(S, m, tri, v);
+        rayTriangle(v, src, dst, m, hit, cbf);
+    }
+    return true;
+}
+
 RSB_HD void rayVsPlane(const ArenaStatic& S, int plane, V3 fromW, V3 toW, RayHit& hit) {
     V3 origin = S.planeOrigin[plane - MAX_MESHES];
     V3 n = S.planeNormal[plane - MAX_MESHES];

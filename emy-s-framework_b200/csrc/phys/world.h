@@ -68,6 +68,24 @@ struct World {
 // world status bits (per-arena status word)
 enum : uint32_t { WS_NONFINITE = 1u, WS_OVERFLOW = 2u, WS_BVH_OVERFLOW = 4u, WS_CULL_MISS = 8u, WS_EPA_OVERFLOW = 16u };
 
+// Index of the lowest set bit of a non-zero mask.
+RSB_HD int lowestBit(uint32_t m) {
+#if defined(__CUDA_ARCH__)
+    return __ffs((int)m) - 1;
+#else
+    return __builtin_ctz(m);
+#endif
+}
+
+// Number of set bits.
+RSB_HD int bitCount(uint32_t m) {
+#if defined(__CUDA_ARCH__)
+    return __popc(m);
+#else
+    return __builtin_popcount(m);
+#endif
+}
+
 // Tolerances of the exact query rejects (Bullet units): the occupancy lookup around a mesh
 // query box or ray segment, and the AABB reject before a ray's convex cast.
 constexpr float kOccTol = 2.f * kUuToBt;
@@ -814,13 +832,18 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
     // meshes with a triangle near the segment: no other mesh can be hit
     const V3 tolv{kOccTol, kOccTol, kOccTol};
     const uint32_t meshNear = occMask(S, vmin(from, to) - tolv, vmax(from, to) + tolv);
+    // the culling state is read once and the test counts kept in registers
+    const bool culled = (W.cull >> rayBody) & 1u, audit = W.cullAudit != 0;
+    uint32_t nRun = 0, nSkip = 0;
+    bool missed = false;
     auto testObj = [&](int o) {
         if (hit.fraction == 0.f) return;
         if (o == ignoreObj) return;
         if (o < MAX_MESHES && !((meshNear >> o) & 1u)) return;
         if (o < NUM_STATICS) {
-            if (cullSkip(W, rayBody)) return;
-            if ((W.cull >> rayBody) & 1u) {
+            if (culled) {
+                nSkip++;
+                if (!audit) return;
                 // audit: would this static have been hit at all?
                 RayHit probe;
                 probe.fraction = 1.f;
@@ -828,8 +851,9 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
                 probe.normal = v3zero();
                 if (o < MAX_MESHES) rayVsMesh(S, o, from, to, probe);
                 else rayVsPlane(S, o, from, to, probe);
-                cullCheck(W, rayBody, probe.obj >= 0);
+                missed |= probe.obj >= 0;
             }
+            nRun++;
             if (o < MAX_MESHES) rayVsMesh(S, o, from, to, hit);
             else rayVsPlane(S, o, from, to, hit);
         } else {
@@ -864,9 +888,15 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
         int i, j, k;
         bpCellIndices(g, from, i, j, k);
         int cell = i * g.cellsY * g.cellsZ + j * g.cellsZ + k;
+        // the statics registered in the cell, in ascending order: meshes (0..15) first, from
+        // the voxel triangle lists when they cover the segment, then the planes
         uint32_t mask = S.bpCells[cell];
-        for (int s = 0; s < NUM_STATICS; s++)
-            if (mask & (1u << s)) testObj(s);
+        const uint32_t meshes = mask & meshNear & ((1u << MAX_MESHES) - 1u);
+        if (meshes && !culled && hit.fraction != 0.f && rayVsMeshesVox(S, meshes, from, to, kOccTol, hit)) {
+            nRun += (uint32_t)bitCount(meshes);
+            mask &= ~((1u << MAX_MESHES) - 1u);
+        }
+        for (; mask; mask &= mask - 1u) testObj(lowestBit(mask));
         // dynamic proxies of the cell in registration order (W.reg is built before the
         // car pre-ticks; see RegOrder)
         const RegOrder& R = W.reg;
@@ -881,6 +911,12 @@ RSB_HD int castRay(const World& W, V3 from, V3 to, int ignoreObj, V3& hitPoint, 
         }
     } else {
         for (int o = 0; o < OBJ_BALL + W.nb; o++) testObj(o);
+    }
+    W.nStatic += nRun;
+    W.nCulled += nSkip;
+    if (missed) {
+        W.nMissed++;
+        W.cullMissed = WS_CULL_MISS;
     }
     if (hit.obj < 0) return -1;
     if (!objIsStatic(hit.obj) && W.b[hit.obj - OBJ_BALL].noResp) return -1;

@@ -44,6 +44,8 @@ struct DevStatic {
     TriEdgeInfo* triInfo = nullptr;
     uint32_t* bpCells = nullptr;
     uint16_t* occ = nullptr;
+    uint32_t* voxOff = nullptr;
+    uint32_t* voxList = nullptr;
     ArenaStatic view{};
 };
 
@@ -345,9 +347,11 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
                 return cudaMemcpy(dst, v.data(), bytes, cudaMemcpyHostToDevice) == cudaSuccess;
             };
             if (!up(D->nodes, H->nodes) || !up(D->subs, H->subs) || !up(D->triVerts, H->triVerts) ||
-                !up(D->triInfo, H->triInfo) || !up(D->bpCells, H->bpCells) || !up(D->occ, H->occ))
+                !up(D->triInfo, H->triInfo) || !up(D->bpCells, H->bpCells) || !up(D->occ, H->occ) ||
+                !up(D->voxOff, H->voxOff) || !up(D->voxList, H->voxList))
                 return fail(nullptr, RSB_ERR_CUDA, "uploading arena meshes failed");
-            D->view = deviceView(*H, D->nodes, D->subs, D->triVerts, D->triInfo, D->bpCells, D->occ);
+            D->view = deviceView(*H, D->nodes, D->subs, D->triVerts, D->triInfo, D->bpCells, D->occ, D->voxOff,
+                                 D->voxList);
             c.dev[key] = D;
             h->stat = D;
         }

@@ -447,6 +447,148 @@ def stress_events(pkg, trained, wl, rank, dev):
             "culled_queries": learned_stats["culled_queries"]}
 
 
+# ------------------------------------------------------------------ GAE over a rollout buffer
+
+GAE_METRIC = "GAE elements/s on 1 B200 (rsb_compute_gae over a flat rollout buffer)"
+GAE_LIB_REF = os.path.join(ROOT, "oracle", "_ref", "libgaeref.so")
+GAE_LIB_PORT = os.path.join(ROOT, "oracle", "_ref", "libgaeoracle.so")
+GAE_PLAYERS, GAE_STEPS = 65536 * 6, 32
+GAE_STD, GAE_CLIP = 1.7, 4.0
+
+
+def gae_rollout(players, steps, seed):
+    """A rollout buffer as the collector lays it out: each player's trajectory contiguous,
+    a goal (NORMAL terminal) with probability 1/300 per step, every trajectory TRUNCATED at
+    the rollout's end; rewards and values standard normal."""
+    rng = np.random.default_rng(seed)
+    term = np.zeros((players, steps), np.int8)
+    term[rng.random((players, steps), dtype=np.float32) < 1.0 / 300.0] = 1
+    term[:, -1] = 2
+    term = term.ravel()
+    T = term.size
+    rews = rng.standard_normal(T, dtype=np.float32)
+    vals = rng.standard_normal(T, dtype=np.float32)
+    trunc = rng.standard_normal(int((term == 2).sum()), dtype=np.float32)
+    return rews, term, vals, trunc
+
+
+def gae_config(players, steps):
+    return {"workload": f"GAE over {players} player trajectories x {steps} env steps (3v3 x 65536 arenas), "
+                        f"player-major, goal terminal p=1/300 per step, truncated at the rollout end; "
+                        f"gamma 0.99, lambda 0.95, returnStd {GAE_STD}, clipRange {GAE_CLIP}",
+            "elements": players * steps, "layout": "flat float32 / int8 buffers in HBM",
+            "l2": "flushed between timed calls (256 MB write); inputs + outputs 264 MB > L2"}
+
+
+def gae_cpu_baseline(rews, term, vals, trunc):
+    """The reference's own CPU recurrence for the device GAE (its parity test's CpuReference,
+    built from the reference tree into oracle/_ref/libgaeref.so), one core, whole buffer; the
+    C restatement of it when that library is absent."""
+    import ctypes as C
+
+    T = len(rews)
+    outs = [np.zeros(T, np.float32) for _ in range(3)]
+    clip = np.zeros(1, np.float32)
+    p = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    if os.path.exists(GAE_LIB_REF):
+        lib = C.CDLL(GAE_LIB_REF)
+        f = lib.gaeref_cpu
+        f.argtypes = [C.c_void_p] * 3 + [C.c_int32, C.c_void_p, C.c_int32, C.c_int32] + [C.c_float] * 4 + \
+            [C.c_void_p] * 4
+        t0 = time.perf_counter()
+        f(p(rews), p(term), p(vals), len(vals), p(trunc), len(trunc), T, 0.99, 0.95, GAE_STD, GAE_CLIP,
+          p(outs[0]), p(outs[1]), p(outs[2]), p(clip))
+        kind = "reference"
+    else:
+        lib = C.CDLL(GAE_LIB_PORT)
+        f = lib.gae_oracle
+        f.argtypes = [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_float] * 4
+        t0 = time.perf_counter()
+        f(p(rews), p(term), p(vals), p(trunc), len(trunc), p(outs[0]), p(outs[1]), p(outs[2]), p(clip), T, 0.99,
+          0.95, GAE_STD, GAE_CLIP)
+        kind = "port"
+    dt = time.perf_counter() - t0
+    return {"value": T / dt, "unit": "elements/s", "cores": 1, "kind": kind,
+            "sample": f"the whole {T}-element buffer once ({dt:.2f} s)"}
+
+
+def run_gae(args, rank, world, dist, steps, warmup, reference_device=False):
+    """Times rsb_compute_gae (or, for the reference arm, the reference's own
+    rsc::ComputeGAEOnDevice built from its tree) on a device-resident rollout buffer."""
+    import ctypes as C
+
+    import torch
+
+    pkg = load_pkg()
+    rsb = pkg.rsb
+    lib = pkg.engine_library()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    rews, term, vals, trunc = gae_rollout(GAE_PLAYERS, GAE_STEPS, 0x5EED0006 + rank)
+    T = len(rews)
+    d_rews, d_term, d_vals, d_trunc = (torch.from_numpy(a).to(dev) for a in (rews, term, vals, trunc))
+    d_out = torch.empty((3, T), dtype=torch.float32, device=dev)
+    d_clip = torch.zeros(1, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    params = rsb.gae_params(lib, return_std=GAE_STD, clip_range=GAE_CLIP)
+    if reference_device:
+        ref = C.CDLL(GAE_LIB_REF)
+        ref.gaeref_device.argtypes = [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 4 + [C.c_int32] + \
+            [C.c_float] * 4 + [C.c_void_p]
+        ref.gaeref_device.restype = C.c_int32
+
+        def call():
+            ref.gaeref_device(d_rews.data_ptr(), d_term.data_ptr(), d_vals.data_ptr(), d_trunc.data_ptr(),
+                              len(trunc), d_out[0].data_ptr(), d_out[1].data_ptr(), d_out[2].data_ptr(),
+                              d_clip.data_ptr(), T, 0.99, 0.95, GAE_STD, GAE_CLIP, sp)
+    else:
+        def call():
+            rsb.compute_gae_device(lib, d_rews.data_ptr(), d_term.data_ptr(), d_vals.data_ptr(), d_trunc.data_ptr(),
+                                   len(trunc), d_out[0].data_ptr(), d_out[1].data_ptr(), d_out[2].data_ptr(),
+                                   d_clip.data_ptr(), T, params, sp)
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            call()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with ClockSampler(dev) as cs:
+        with torch.cuda.stream(stream):
+            for e0, e1 in events:
+                flush.fill_(1.0)
+                e0.record(stream)
+                call()
+                e1.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    times = [e0.elapsed_time(e1) for e0, e1 in events]
+    ms = reduce_max(statistics.mean(times), dist, dev)
+    alg_bytes = T * (4 + 1 + 4 + 3 * 4) + 4 * len(trunc) + 4
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    res = {"value": T * world / (ms / 1e3), "unit": "elements/s", "ms_per_call": ms, "elements": T,
+           "roofline": {"bound": "hbm", "kernel": "gaeSegmentKernel (+ summary and scan)", "achieved": achieved,
+                        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                        "peak_kind": peak_kind, "bytes_per_call": alg_bytes},
+           "gpu_launches": 3 * steps, "clocks": cs.summary()}
+    if not reference_device:
+        # e2e through the host entry point: copies in, kernels, copies out
+        e2e = []
+        for _ in range(max(3, min(steps, 5))):
+            t0 = time.perf_counter()
+            rsb.compute_gae(lib, rews, term, vals, trunc, params)
+            e2e.append(time.perf_counter() - t0)
+        res["e2e"] = {"value": T * world / reduce_max(statistics.median(e2e), dist, dev), "unit": "elements/s",
+                      "h2d_bytes_per_step": T * 9 + 4 * len(trunc), "d2h_bytes_per_step": T * 12 + 4}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res["cpu_baseline"] = gae_cpu_baseline(rews, term, vals, trunc)
+    return res
+
+
 # ------------------------------------------------------------------ CPU reference
 
 def cpu_reference(args, sample_s=10.0, threads=None):
@@ -489,7 +631,25 @@ def cpu_reference(args, sample_s=10.0, threads=None):
                                           f"incl. obs/masks/rewards/terminals/resets ({dt:.1f} s)"}
 
 
+def gae_line(args, res, world, impl=None):
+    line = {"metric": GAE_METRIC, "value": res["value"], "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["ms_per_call"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded rollout buffer)",
+            "config": gae_config(GAE_PLAYERS, GAE_STEPS)} | {k: v for k, v in res.items() if k not in (
+                "value", "unit", "ms_per_call")}
+    if impl:
+        line["impl"] = impl
+    return line
+
+
 def run_reference(args):
+    if args.config == "gae":
+        # the reference's own implementation of this path is its device GAE
+        # (RocketSimCuda/src/GAECuda.cu), built from its tree for sm_100a
+        res = run_gae(args, 0, 1, None, args.steps, args.warmup, reference_device=True)
+        line = gae_line(args, res, args.gpus, impl="reference")
+        line["e2e"] = {"value": res["value"], "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        return line
     cb = cpu_reference(args, sample_s=args.ref_seconds)
     wl = Workload(args)
     return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "arena-ticks/s",
@@ -505,7 +665,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c3", choices=sorted(PRESETS))
+    ap.add_argument("--config", default="c3", choices=sorted(PRESETS) + ["gae"])
     ap.add_argument("--arenas", type=int, default=None)
     ap.add_argument("--team-size", type=int, default=None)
     ap.add_argument("--tick-skip", type=int, default=8)
@@ -515,6 +675,7 @@ def main():
     ap.add_argument("--cull", default=None, choices=["learned", "exact"])
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gae", action="store_true", help="skip the GAE measurement of the c3 line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -532,7 +693,17 @@ def main():
 
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = dist_mod
+    if args.config == "gae":
+        res = gae_line(args, run_gae(args, rank, world, dist, args.steps, args.warmup), world)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     res = run_ours(args, rank, world, dist)
+    # the next stage of the rollout: GAE over a rollout buffer of this size, device-resident
+    if args.config == "c3" and not args.no_gae:
+        res["gae"] = run_gae(args, rank, world, dist, steps=10, warmup=3)
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             res["cpu_baseline"] = cpu_reference(args, sample_s=args.ref_seconds)

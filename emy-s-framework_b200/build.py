@@ -20,7 +20,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["rsb_engine.cu"]
+CU_SOURCES = ["rsb_engine.cu", "gae.cu"]
 CPP_SOURCES = ["arena_build.cpp"]
 
 

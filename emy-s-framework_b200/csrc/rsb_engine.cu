@@ -1052,6 +1052,11 @@ rsb_status rsb_culler_train(rsb_handle* h, const rsb_culler_config* cfg, rsb_cul
     return RSB_OK;
 }
 
+namespace rsb {
+// Message of a failed call that has no handle (rsb_last_error with h == NULL returns it).
+void setGlobalError(const std::string& msg) { g_createError = msg; }
+}  // namespace rsb
+
 extern "C" {
 
 rsb_status rsb_last_error(const rsb_handle* h, char* buf, size_t n) {

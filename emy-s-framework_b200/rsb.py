@@ -158,6 +158,10 @@ class Stats(C.Structure):
         "solver_rows", "arenas_reverted", "status_bits_seen", "state_bytes_per_step")]
 
 
+class GaeParams(C.Structure):
+    _fields_ = [("gamma", C.c_float), ("lam", C.c_float), ("return_std", C.c_float), ("clip_range", C.c_float)]
+
+
 CAR_DTYPE = np.dtype(CarState)
 BALL_DTYPE = np.dtype(BallState)
 PAD_DTYPE = np.dtype(PadState)
@@ -206,6 +210,9 @@ _SIGS = {
     "rsb_get_pads": [_P, _P, C.c_int32],
     "rsb_set_pads": [_P, _P, C.c_int32],
     "rsb_get_arena_info": [_P, _P, C.c_int32],
+    "rsb_gae_default_params": [_P],
+    "rsb_compute_gae": [_P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, C.c_int32, _P, _P],
+    "rsb_compute_gae_host": [_P, _P, _P, C.c_int32, _P, C.c_int32, _P, _P, _P, _P, C.c_int32, _P],
     "rsb_sync": [_P],
     "rsb_stats_get": [_P, C.POINTER(Stats)],
     "rsb_last_error": [_P, C.c_char_p, C.c_size_t],
@@ -260,6 +267,60 @@ def default_action_lut(lib: C.CDLL) -> np.ndarray:
     if st != 0:
         raise RsbError(st, "rsb_default_action_lut failed")
     return lut
+
+
+def gae_params(lib: C.CDLL, gamma: float | None = None, lam: float | None = None, return_std: float | None = None,
+               clip_range: float | None = None) -> GaeParams:
+    """rsb_gae_default_params (gamma 0.99, lambda 0.95, no standardisation), then overrides."""
+    p = GaeParams()
+    st = lib.rsb_gae_default_params(C.byref(p))
+    if st != 0:
+        raise RsbError(st, "rsb_gae_default_params failed")
+    for k, v in (("gamma", gamma), ("lam", lam), ("return_std", return_std), ("clip_range", clip_range)):
+        if v is not None:
+            setattr(p, k, v)
+    return p
+
+
+def compute_gae_device(lib: C.CDLL, rews: int, terminals: int, val_preds: int, trunc_val_preds: int,
+                       num_truncs: int, advantages: int, target_values: int, returns: int, rew_clip_portion: int,
+                       T: int, params: GaeParams, stream: int = 0):
+    """rsb_compute_gae on device pointers (ints), the drop-in for rsc::ComputeGAEOnDevice
+    (RocketSimCuda/include/RocketSimCudaTraining.h:17-30): float32 rewards / values, int8
+    terminals (1 NORMAL, 2 TRUNCATED), val_preds[T] read when the final step is not terminal."""
+    st = lib.rsb_compute_gae(_P(rews or None), _P(terminals or None), _P(val_preds or None),
+                             _P(trunc_val_preds or None), num_truncs, _P(advantages or None),
+                             _P(target_values or None), _P(returns or None), _P(rew_clip_portion or None), T,
+                             C.byref(params), _P(stream or None))
+    if st != 0:
+        raise RsbError(st, _global_error(lib))
+
+
+def compute_gae(lib: C.CDLL, rews, terminals, val_preds, trunc_val_preds=None, params: GaeParams | None = None):
+    """rsb_compute_gae_host on numpy arrays: (advantages, target_values, returns, rew_clip_portion).
+    Same arguments as the learner's GAE::Compute (GigaLearnCPP/src/private/GigaLearnCPP/PPO/GAE.h:8-12)
+    but the device function's conventions (truncation values counted from the buffer's end)."""
+    r = np.ascontiguousarray(rews, np.float32)
+    t = np.ascontiguousarray(terminals, np.int8)
+    v = np.ascontiguousarray(val_preds, np.float32)
+    tv = np.ascontiguousarray(trunc_val_preds if trunc_val_preds is not None else np.zeros(0), np.float32)
+    n = len(r)
+    if len(t) != n:
+        raise ValueError("rews and terminals differ in length")
+    params = params or gae_params(lib)
+    adv, tgt, ret = (np.empty(n, np.float32) for _ in range(3))
+    clip = np.zeros(1, np.float32)
+    st = lib.rsb_compute_gae_host(_ptr(r), _ptr(t), _ptr(v), len(v), _ptr(tv) if len(tv) else None, len(tv),
+                                  _ptr(adv), _ptr(tgt), _ptr(ret), _ptr(clip), n, C.byref(params))
+    if st != 0:
+        raise RsbError(st, _global_error(lib))
+    return adv, tgt, ret, float(clip[0])
+
+
+def _global_error(lib: C.CDLL) -> str:
+    buf = C.create_string_buffer(512)
+    lib.rsb_last_error(None, buf, len(buf))
+    return buf.value.decode(errors="replace")
 
 
 def default_action_table() -> np.ndarray:

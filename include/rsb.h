@@ -367,6 +367,46 @@ rsb_status rsb_culler_predict(rsb_handle* h, const float* pts, int32_t n, float*
 rsb_status rsb_culler_gradients(rsb_handle* h, const float* pts, const float* target, int32_t n,
                                 float over_weight, float* grad, float* loss);
 
+/* ---- GAE over a flat rollout buffer (no handle) ----
+ * rsb_compute_gae replaces rsc::ComputeGAEOnDevice (RocketSimCuda/include/
+ * RocketSimCudaTraining.h:17-30, RocketSimCuda/src/GAECuda.cu:247-300) with the same
+ * arguments in the same order and the same results element for element:
+ *   - terminals: 0 running, 1 NORMAL (episode end, bootstrap 0), 2 TRUNCATED (bootstrap from
+ *     trunc_val_preds); every nonzero value ends an independent segment;
+ *   - the k-th TRUNCATED step counted from the END of the buffer (k = 0 for the last one)
+ *     bootstraps from trunc_val_preds[k] (the learner's CPU GAE::Compute,
+ *     GigaLearnCPP/src/private/GigaLearnCPP/PPO/GAE.cpp:164, indexes them the other way
+ *     round); a num_truncs that does not match the TRUNCATED steps reads nothing out of range
+ *     (such a step bootstraps from 0);
+ *   - val_preds holds T values, and one more (val_preds[T]) when terminals[T-1] == 0: the
+ *     final step then bootstraps from it, as the reference does;
+ *   - advantages, returns and target_values (= val_preds + advantages) are written for all T
+ *     elements; *rew_clip_portion = (sum|r/std| - sum|clip(r/std)|) / max(sum|r/std|, 1e-7),
+ *     summed in another order than the reference's atomics (equal within float rounding).
+ * All pointers are device pointers; stream is a cudaStream_t as void* (NULL = legacy default
+ * stream).  The library keeps a small per-device scratch (grown on demand, as the
+ * reference's is); calls on one device are serialised on the host, and work queued on two
+ * streams must not overlap.  Three kernel launches, no host synchronisation. */
+typedef struct rsb_gae_params {
+    float gamma;       /* 0.99 by default */
+    float lambda;      /* 0.95 */
+    float return_std;  /* > 0: rewards are divided by it (and clipped to +-clip_range if > 0) */
+    float clip_range;
+} rsb_gae_params;
+
+rsb_status rsb_gae_default_params(rsb_gae_params* out);
+rsb_status rsb_compute_gae(const float* rews, const int8_t* terminals, const float* val_preds,
+                           const float* trunc_val_preds, int32_t num_truncs, float* advantages,
+                           float* target_values, float* returns, float* rew_clip_portion, int32_t T,
+                           const rsb_gae_params* params, void* stream);
+/* The same on host buffers (the call site of the learner's CPU GAE::Compute,
+ * GAE.h:8-12): copies in, computes on the current device, copies out, synchronises.
+ * num_val_preds >= T, and >= T + 1 when terminals[T-1] == 0. */
+rsb_status rsb_compute_gae_host(const float* rews, const int8_t* terminals, const float* val_preds,
+                                int32_t num_val_preds, const float* trunc_val_preds, int32_t num_truncs,
+                                float* advantages, float* target_values, float* returns,
+                                float* rew_clip_portion, int32_t T, const rsb_gae_params* params);
+
 rsb_status rsb_sync(rsb_handle* h);
 rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out);
 /* Copies the last error message (NUL-terminated, truncated to n). Safe with h == NULL

@@ -485,6 +485,25 @@ rsb_status rsb_culler_distance(rsb_handle* h, const float*, int32_t, float*) { r
 rsb_status rsb_culler_predict(rsb_handle* h, const float*, int32_t, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 rsb_status rsb_culler_gradients(rsb_handle* h, const float*, const float*, int32_t, float, float*, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 
+// GAE lives in its own oracle libraries (gae_oracle.c, gae_pin.cpp); this one only answers
+// the ABI.
+rsb_status rsb_gae_default_params(rsb_gae_params* out) {
+    if (!out) return RSB_ERR_INVALID;
+    out->gamma = 0.99f;
+    out->lambda = 0.95f;
+    out->return_std = 0.f;
+    out->clip_range = 0.f;
+    return RSB_OK;
+}
+rsb_status rsb_compute_gae(const float*, const int8_t*, const float*, const float*, int32_t, float*, float*, float*,
+                           float*, int32_t, const rsb_gae_params*, void*) {
+    return RSB_ERR_UNSUPPORTED;
+}
+rsb_status rsb_compute_gae_host(const float*, const int8_t*, const float*, int32_t, const float*, int32_t, float*,
+                                float*, float*, float*, int32_t, const rsb_gae_params*) {
+    return RSB_ERR_UNSUPPORTED;
+}
+
 // The CPU oracle has a single configuration.
 rsb_status rsb_autotune(rsb_handle* h, int32_t, rsb_tune_entry*, int32_t, int32_t* count) {
     if (!h) return RSB_ERR_INVALID;

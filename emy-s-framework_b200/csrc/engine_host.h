@@ -186,17 +186,17 @@ inline void cellOf(const ArenaStatic& S, V3 mn, int32_t& cell, int32_t& ci, int3
 }
 
 // RocketSim RotMat holds forward, right, up as the basis columns
-inline M3 basisFromRot(const rsb_rotmat& r) {
+RSB_HD M3 basisFromRot(const rsb_rotmat& r) {
     return m3(r.forward.x, r.right.x, r.up.x, r.forward.y, r.right.y, r.up.y, r.forward.z, r.right.z, r.up.z);
 }
-inline rsb_rotmat rotFromBasis(const float* rot) {
+RSB_HD rsb_rotmat rotFromBasis(const float* rot) {
     rsb_rotmat r;
     r.forward = rsb_vec3{rot[0], rot[3], rot[6]};
     r.right = rsb_vec3{rot[1], rot[4], rot[7]};
     r.up = rsb_vec3{rot[2], rot[5], rot[8]};
     return r;
 }
-inline void basisToFloats(const M3& b, float* rot) {
+RSB_HD void basisToFloats(const M3& b, float* rot) {
     for (int i = 0; i < 3; i++) {
         rot[3 * i + 0] = b.r[i].x;
         rot[3 * i + 1] = b.r[i].y;
@@ -318,7 +318,7 @@ inline void initRecords(const ArenaStatic& S, const WorldParams& P, const std::v
     }
 }
 
-inline rsb_controls ctlFromRecord(const CarP& p) {
+RSB_HD rsb_controls ctlFromRecord(const CarP& p) {
     rsb_controls r{};
     r.throttle = p.lastCtl[0];
     r.steer = p.lastCtl[1];
@@ -332,7 +332,7 @@ inline rsb_controls ctlFromRecord(const CarP& p) {
 }
 
 // Car::GetState
-inline rsb_car_state carStateOf(const CarP& p, uint32_t id) {
+RSB_HD rsb_car_state carStateOf(const CarP& p, uint32_t id) {
     rsb_car_state o{};
     V3 pos = V3{p.pos[0], p.pos[1], p.pos[2]} * kBtToUu;
     V3 vel = V3{p.lin[0], p.lin[1], p.lin[2]} * kBtToUu;
@@ -380,8 +380,9 @@ inline rsb_car_state carStateOf(const CarP& p, uint32_t id) {
 }
 
 // Car::SetState: transform, velocities and the whole CarState replaced; the broadphase
-// registration and the vehicle's wheel values are kept
-inline void applyCarState(CarP& p, const rsb_car_state& s) {
+// registration and the vehicle's wheel values are kept (host and device: the state ring's
+// restore kernel applies it too)
+RSB_HD void applyCarState(CarP& p, const rsb_car_state& s) {
     M3 b = basisFromRot(s.rot);
     Xf x{b, V3{s.pos.x, s.pos.y, s.pos.z} * kUuToBt};
     xfToP(x, p.pos, p.rot);
@@ -433,7 +434,7 @@ inline void applyCarState(CarP& p, const rsb_car_state& s) {
     p.lastCtlBits = (lc.jump ? 1u : 0u) | (lc.boost ? 2u : 0u) | (lc.handbrake ? 4u : 0u);
 }
 
-inline rsb_ball_state ballStateOf(const BallP& p) {
+RSB_HD rsb_ball_state ballStateOf(const BallP& p) {
     rsb_ball_state o{};
     V3 pos = V3{p.pos[0], p.pos[1], p.pos[2]} * kBtToUu;
     V3 vel = V3{p.lin[0], p.lin[1], p.lin[2]} * kBtToUu;
@@ -444,7 +445,7 @@ inline rsb_ball_state ballStateOf(const BallP& p) {
     return o;
 }
 
-inline void applyBallState(BallP& p, const rsb_ball_state& s) {
+RSB_HD void applyBallState(BallP& p, const rsb_ball_state& s) {
     Xf x{basisFromRot(s.rot), V3{s.pos.x, s.pos.y, s.pos.z} * kUuToBt};
     xfToP(x, p.pos, p.rot);
     V3 v = V3{s.vel.x, s.vel.y, s.vel.z} * kUuToBt;

@@ -130,6 +130,19 @@ struct rsb_handle {
     RewardParams rewardParams{};
     std::string err;
     rsb_stats stats{};
+    // state ring (rsb_ring_*)
+    struct Ring {
+        bool enabled = false, replayDisabled = false;
+        rsb_ring_config cfg{};
+        uint32_t rng = 0xA5A5A5A5u;
+        uint32_t* dSlots = nullptr;  // depth slots, each [ball planes | car planes | pad planes]
+        size_t slotWords = 0;
+        int writeIdx = 0, filled = 0, stepsSinceCapture = 0;
+        uint64_t captures = 0, restores = 0, restoreCalls = 0;
+        uint32_t* dJobs = nullptr;   // per rewound arena: its index and the xorshift state of its first draw
+        int jobCap = 0;
+        std::vector<uint32_t> jobs;
+    } ring;
 };
 
 static rsb_status fail(rsb_handle* h, rsb_status code, const std::string& msg) {
@@ -164,6 +177,78 @@ static const StepVariant kStepVariants[] = {{stepKernel<1>, 1}, {stepKernel<3>, 
 constexpr int kNumStepVariants = sizeof(kStepVariants) / sizeof(kStepVariants[0]);
 static const int kStepBlocks[] = {32, 64, 128};
 constexpr int kNumStepBlocks = sizeof(kStepBlocks) / sizeof(kStepBlocks[0]);
+
+// xorshift32 draw in [0, 1] and range of the reference's state ring (CudaEnvSet.cpp:608-617)
+RSB_HD float ringRand01(uint32_t& rng) {
+    rng ^= rng << 13;
+    rng ^= rng >> 17;
+    rng ^= rng << 5;
+    return (rng & 0xFFFFFFu) / float(0xFFFFFFu);
+}
+RSB_HD float ringRange(uint32_t& rng, float lo, float hi) { return lo + (hi - lo) * ringRand01(rng); }
+
+// Rewinds the listed arenas to a ring slot (ApplyArenaSnap, CudaEnvSet.cpp:698-753): for each
+// car the slot's public state (Car::GetState) jittered and written over the live car as
+// Car::SetState writes it, then the ball, then the pads (their public fields).  One thread per
+// listed arena; jobs[2 j] = arena, jobs[2 j + 1] = xorshift state of its first draw.
+__global__ void ringRestoreKernel(uint32_t* ball, uint32_t* car, uint32_t* pad, uint32_t* arena,
+                                  const int32_t* teamSize, const uint32_t* sBall, const uint32_t* sCar,
+                                  const uint32_t* sPad, const uint32_t* jobs, int n, int N, float fp, float fv,
+                                  float goalLine) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int a = (int)jobs[2 * j];
+    uint32_t rng = jobs[2 * j + 1];
+    const int cars = 2 * teamSize[a];
+    for (int s = 0; s < cars; s++) {
+        CarP live, snap;
+        loadPlanes(live, car, s * N + a, MAX_CARS * N);
+        loadPlanes(snap, sCar, s * N + a, MAX_CARS * N);
+        rsb_car_state st = carStateOf(snap, (uint32_t)s + 1u);
+        if (fp > 0.f) {
+            st.pos.x += ringRange(rng, -fp, fp);
+            st.pos.y += ringRange(rng, -fp, fp);
+            const float z = st.pos.z + ringRange(rng, -fp * 0.25f, fp * 0.35f);
+            st.pos.z = 17.f < z ? z : 17.f;
+        }
+        if (fv > 0.f) {
+            st.vel.x += ringRange(rng, -fv, fv);
+            st.vel.y += ringRange(rng, -fv, fv);
+            st.vel.z += ringRange(rng, -fv * 0.5f, fv * 0.5f);
+        }
+        applyCarState(live, st);
+        storePlanes(live, car, s * N + a, MAX_CARS * N);
+    }
+    BallP live, snap;
+    loadPlanes(live, ball, a, N);
+    loadPlanes(snap, sBall, a, N);
+    rsb_ball_state bs = ballStateOf(snap);
+    if (fp > 0.f) {
+        bs.pos.x += ringRange(rng, -fp, fp);
+        bs.pos.y += ringRange(rng, -fp, fp);
+        const float z = bs.pos.z + ringRange(rng, -fp * 0.2f, fp * 0.4f);
+        bs.pos.z = 93.f < z ? z : 93.f;
+    }
+    if (fv > 0.f) {
+        bs.vel.x += ringRange(rng, -fv, fv);
+        bs.vel.y += ringRange(rng, -fv, fv);
+        bs.vel.z += ringRange(rng, -fv * 0.5f, fv * 0.5f);
+    }
+    applyBallState(live, bs);
+    storePlanes(live, ball, a, N);
+    // the goal-line flag follows the new ball position, as rsb_set_balls keeps it
+    ArenaP ap;
+    loadPlanes(ap, arena, a, N);
+    const float y = live.pos[1] * kBtToUu;
+    ap.scored = fabsf(y) > goalLine ? (live.pos[1] > 0 ? 1 : 2) : 0;
+    storePlanes(ap, arena, a, N);
+    for (int p = 0; p < NUM_PADS; p++) {
+        PadP pp;
+        loadPlanes(pp, sPad, p * N + a, N * NUM_PADS);
+        pp.bits = (pp.bits & 1u) | ((pp.bits >> 8) << 8);  // is_active and prev_locked_car_id
+        storePlanes(pp, pad, p * N + a, N * NUM_PADS);
+    }
+}
 
 __global__ void expandActionsKernel(const int32_t* idx, const rsb_controls* lut, int lutCount, rsb_controls* out, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -417,6 +502,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
     cudaFree(h->dTris);
     cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
+    cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return RSB_OK;
@@ -1051,6 +1137,163 @@ rsb_status rsb_culler_train(rsb_handle* h, const rsb_culler_config* cfg, rsb_cul
     }
     return RSB_OK;
 }
+
+// ------------------------------------------------------------------ state ring
+
+extern "C" {
+
+rsb_status rsb_ring_default_config(rsb_ring_config* out) {
+    if (!out) return RSB_ERR_INVALID;
+    out->depth = 10;
+    out->capture_every = 3;
+    out->restore_fraction = 0.05f;
+    out->max_arenas_per_restore = 64;
+    out->fuzz_pos = 25.f;
+    out->fuzz_vel = 80.f;
+    out->lookback_slots = 7;
+    out->seed = 0xA5A5A5A5u;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_configure(rsb_handle* h, const rsb_ring_config* cfg) {
+    if (!h || !cfg) return fail(h, RSB_ERR_INVALID, "rsb_ring_configure: null argument");
+    RSB_CUDA(cudaSetDevice(h->device));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    auto& R = h->ring;
+    cudaFree(R.dSlots);
+    R.dSlots = nullptr;
+    R.enabled = false;
+    R.filled = R.writeIdx = R.stepsSinceCapture = 0;
+    if (cfg->depth <= 0 || h->N <= 0) return RSB_OK;
+    R.cfg = *cfg;
+    R.cfg.depth = std::max(2, cfg->depth);
+    R.cfg.capture_every = std::max(1, cfg->capture_every);
+    R.cfg.lookback_slots = std::max(1, std::min(cfg->lookback_slots, R.cfg.depth - 1));
+    R.cfg.restore_fraction =
+        std::max(0.01f, std::min(0.05f, cfg->restore_fraction > 0.f ? cfg->restore_fraction : 0.05f));
+    R.cfg.max_arenas_per_restore = std::max(1, cfg->max_arenas_per_restore > 0 ? cfg->max_arenas_per_restore : 64);
+    R.rng = cfg->seed ? cfg->seed : 0xA5A5A5A5u;
+    R.slotWords = (size_t)W_BALL * h->N + (size_t)W_CAR * MAX_CARS * h->N + (size_t)W_PAD * NUM_PADS * h->N;
+    const size_t bytes = (size_t)R.cfg.depth * R.slotWords * sizeof(uint32_t);
+    if (cudaMalloc(&R.dSlots, bytes) != cudaSuccess) {
+        R.dSlots = nullptr;
+        cudaGetLastError();
+        return fail(h, RSB_ERR_NOMEM, "rsb_ring_configure: cannot allocate " + std::to_string(bytes) + " bytes of slots");
+    }
+    R.enabled = true;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_capture(rsb_handle* h, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    auto& R = h->ring;
+    if (!R.enabled) return RSB_OK;
+    RSB_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    uint32_t* slot = R.dSlots + (size_t)R.writeIdx * R.slotWords;
+    const size_t nb = (size_t)W_BALL * h->N, nc = (size_t)W_CAR * MAX_CARS * h->N, np = (size_t)W_PAD * NUM_PADS * h->N;
+    RSB_CUDA(cudaMemcpyAsync(slot, h->dBall, nb * 4, cudaMemcpyDeviceToDevice, st));
+    RSB_CUDA(cudaMemcpyAsync(slot + nb, h->dCar, nc * 4, cudaMemcpyDeviceToDevice, st));
+    RSB_CUDA(cudaMemcpyAsync(slot + nb + nc, h->dPad, np * 4, cudaMemcpyDeviceToDevice, st));
+    R.writeIdx = (R.writeIdx + 1) % R.cfg.depth;
+    if (R.filled < R.cfg.depth) R.filled++;
+    R.captures++;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_maybe_capture(rsb_handle* h, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    auto& R = h->ring;
+    if (!R.enabled) return RSB_OK;
+    if (++R.stepsSinceCapture < R.cfg.capture_every) return RSB_OK;
+    R.stepsSinceCapture = 0;
+    return rsb_ring_capture(h, stream);
+}
+
+rsb_status rsb_ring_restore(rsb_handle* h, float restore_fraction, int32_t lookback_slots, float fuzz_scale,
+                            int32_t max_arenas, int32_t* restored, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    if (restored) *restored = 0;
+    auto& R = h->ring;
+    if (!R.enabled || R.replayDisabled || R.filled < 2) return RSB_OK;
+    const int N = h->N;
+    float frac = restore_fraction >= 0.f ? restore_fraction : R.cfg.restore_fraction;
+    frac = std::max(0.01f, std::min(0.05f, frac));
+    int lookback = lookback_slots >= 0 ? lookback_slots : R.cfg.lookback_slots;
+    lookback = std::max(1, std::min(lookback, R.filled - 1));
+    int lastWritten = R.writeIdx - 1;
+    if (lastWritten < 0) lastWritten = R.cfg.depth - 1;
+    int slot = lastWritten - lookback;
+    while (slot < 0) slot += R.cfg.depth;
+    int cap = max_arenas > 0 ? max_arenas : R.cfg.max_arenas_per_restore;
+    if (cap <= 0) cap = 64;
+    const int fivePct = std::max(1, (int)std::lround(0.05 * (double)N));
+    cap = std::min(cap, fivePct);
+    int nRestore = std::max(1, (int)std::lround(frac * (double)N));
+    nRestore = std::min(nRestore, N);
+    nRestore = std::min(nRestore, cap);
+    // partial Fisher-Yates over the arena indices, then each arena's jitter draws in order
+    std::vector<int> order((size_t)N);
+    for (int i = 0; i < N; i++) order[(size_t)i] = i;
+    for (int i = 0; i < nRestore; i++) {
+        int j = i + (int)(ringRand01(R.rng) * (N - i));
+        if (j >= N) j = N - 1;
+        std::swap(order[(size_t)i], order[(size_t)j]);
+    }
+    const float fp = R.cfg.fuzz_pos * fuzz_scale;
+    const float fv = R.cfg.fuzz_vel * fuzz_scale;
+    const int drawsPerBody = (fp > 0.f ? 3 : 0) + (fv > 0.f ? 3 : 0);
+    R.jobs.resize(2 * (size_t)nRestore);
+    for (int i = 0; i < nRestore; i++) {
+        const int a = order[(size_t)i];
+        R.jobs[2 * (size_t)i] = (uint32_t)a;
+        R.jobs[2 * (size_t)i + 1] = R.rng;
+        const int draws = (2 * h->teamSize[(size_t)a] + 1) * drawsPerBody;
+        for (int k = 0; k < draws; k++) ringRand01(R.rng);
+    }
+    RSB_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    if (R.jobCap < nRestore) {
+        if (R.dJobs) {
+            RSB_CUDA(cudaStreamSynchronize(st));
+            cudaFree(R.dJobs);
+            R.dJobs = nullptr;
+        }
+        R.jobCap = 0;
+        const int capJobs = std::max(nRestore, 64);
+        RSB_CUDA(cudaMalloc(&R.dJobs, 2 * sizeof(uint32_t) * (size_t)capJobs));
+        R.jobCap = capJobs;
+    }
+    RSB_CUDA(cudaMemcpyAsync(R.dJobs, R.jobs.data(), R.jobs.size() * 4, cudaMemcpyHostToDevice, st));
+    const uint32_t* sBall = R.dSlots + (size_t)slot * R.slotWords;
+    const uint32_t* sCar = sBall + (size_t)W_BALL * N;
+    const uint32_t* sPad = sCar + (size_t)W_CAR * MAX_CARS * N;
+    ringRestoreKernel<<<(nRestore + 63) / 64, 64, 0, st>>>(h->dBall, h->dCar, h->dPad, h->dArena, h->dTeamSize, sBall,
+                                                            sCar, sPad, R.dJobs, nRestore, N, fp, fv,
+                                                            h->P.goalBaseY + h->P.ballRadiusUu);
+    RSB_CUDA(cudaGetLastError());
+    R.restores += (uint64_t)nRestore;
+    R.restoreCalls++;
+    // the reference's tripwire: far more restores than captures turns replay off
+    if (R.restoreCalls > 32 && R.captures > 0 && R.restoreCalls > R.captures * 4) R.replayDisabled = true;
+    if (restored) *restored = nRestore;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_stats_get(rsb_handle* h, rsb_ring_stats* out) {
+    if (!h || !out) return RSB_ERR_INVALID;
+    const auto& R = h->ring;
+    out->depth = R.enabled ? R.cfg.depth : 0;
+    out->filled = R.filled;
+    out->write_idx = R.writeIdx;
+    out->replay_disabled = R.replayDisabled ? 1 : 0;
+    out->captures = R.captures;
+    out->restores = R.restores;
+    out->restore_calls = R.restoreCalls;
+    return RSB_OK;
+}
+
+}  // extern "C"
 
 namespace rsb {
 // Message of a failed call that has no handle (rsb_last_error with h == NULL returns it).

@@ -158,6 +158,18 @@ class Stats(C.Structure):
         "solver_rows", "arenas_reverted", "status_bits_seen", "state_bytes_per_step")]
 
 
+class RingConfig(C.Structure):
+    _fields_ = [("depth", C.c_int32), ("capture_every", C.c_int32), ("restore_fraction", C.c_float),
+                ("max_arenas_per_restore", C.c_int32), ("fuzz_pos", C.c_float), ("fuzz_vel", C.c_float),
+                ("lookback_slots", C.c_int32), ("seed", C.c_uint32)]
+
+
+class RingStats(C.Structure):
+    _fields_ = [("depth", C.c_int32), ("filled", C.c_int32), ("write_idx", C.c_int32),
+                ("replay_disabled", C.c_int32), ("captures", C.c_uint64), ("restores", C.c_uint64),
+                ("restore_calls", C.c_uint64)]
+
+
 class GaeParams(C.Structure):
     _fields_ = [("gamma", C.c_float), ("lam", C.c_float), ("return_std", C.c_float), ("clip_range", C.c_float)]
 
@@ -210,6 +222,12 @@ _SIGS = {
     "rsb_get_pads": [_P, _P, C.c_int32],
     "rsb_set_pads": [_P, _P, C.c_int32],
     "rsb_get_arena_info": [_P, _P, C.c_int32],
+    "rsb_ring_default_config": [_P],
+    "rsb_ring_configure": [_P, _P],
+    "rsb_ring_capture": [_P, _P],
+    "rsb_ring_maybe_capture": [_P, _P],
+    "rsb_ring_restore": [_P, C.c_float, C.c_int32, C.c_float, C.c_int32, C.POINTER(C.c_int32), _P],
+    "rsb_ring_stats_get": [_P, _P],
     "rsb_gae_default_params": [_P],
     "rsb_compute_gae": [_P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, C.c_int32, _P, _P],
     "rsb_compute_gae_host": [_P, _P, _P, C.c_int32, _P, C.c_int32, _P, _P, _P, _P, C.c_int32, _P],
@@ -518,6 +536,36 @@ class Batch:
         self._check(self.lib.rsb_culler_gradients(self._h, _ptr(p), _ptr(t), len(p), over_weight, _ptr(g),
                                                   C.byref(loss)))
         return g, loss.value
+
+    # ---------------------------------------------------------------- state ring
+    def ring_configure(self, **overrides) -> RingConfig:
+        """rsb_ring_configure with the reference's defaults (depth 10, capture every 3 env
+        steps, 5 % of the arenas, 25 uu / 80 uu/s jitter, 7 slots back) and the given fields."""
+        cfg = RingConfig()
+        self._check(self.lib.rsb_ring_default_config(C.byref(cfg)))
+        for k, v in overrides.items():
+            setattr(cfg, k, v)
+        self._ring_cfg = cfg
+        self._check(self.lib.rsb_ring_configure(self._h, C.byref(cfg)))
+        return cfg
+
+    def ring_capture(self, stream: int | None = None):
+        self._check(self.lib.rsb_ring_capture(self._h, C.c_void_p(stream or 0)))
+
+    def ring_maybe_capture(self, stream: int | None = None):
+        self._check(self.lib.rsb_ring_maybe_capture(self._h, C.c_void_p(stream or 0)))
+
+    def ring_restore(self, restore_fraction: float = -1.0, lookback_slots: int = -1, fuzz_scale: float = 1.0,
+                     max_arenas: int = -1, stream: int | None = None) -> int:
+        n = C.c_int32()
+        self._check(self.lib.rsb_ring_restore(self._h, restore_fraction, lookback_slots, fuzz_scale, max_arenas,
+                                              C.byref(n), C.c_void_p(stream or 0)))
+        return n.value
+
+    def ring_stats(self) -> dict:
+        st = RingStats()
+        self._check(self.lib.rsb_ring_stats_get(self._h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in RingStats._fields_}
 
     def sync(self):
         self._check(self.lib.rsb_sync(self._h))

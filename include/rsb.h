@@ -367,6 +367,54 @@ rsb_status rsb_culler_predict(rsb_handle* h, const float* pts, int32_t n, float*
 rsb_status rsb_culler_gradients(rsb_handle* h, const float* pts, const float* target, int32_t n,
                                 float over_weight, float* grad, float* loss);
 
+/* ---- state ring: rewind a few arenas to an earlier state ----
+ * Replaces the state ring of GGL::CudaEnvSet (GigaLearnCPP/src/public/GigaLearnCPP/Sim/
+ * CudaEnvSet.h:100-125, CudaEnvSet.cpp:608-815).  The reference copies every car, ball and
+ * pad state to the host at each capture (a device synchronisation plus a full-batch
+ * download); here the slots live in device memory and a capture is three device-to-device
+ * copies on the stream.  A restore picks the arenas and draws the position / velocity
+ * jitter exactly as RestoreStateRingReplay / ApplyArenaSnap do (xorshift32 stream,
+ * partial Fisher-Yates over the arena indices, cars then ball), then applies, on the
+ * device, what the reference's SetCarState / SetBallState / SetBoostPadStates would: the
+ * public state of the slot, jittered, written over the live arena (broadphase registration
+ * and wheel values of the live cars are kept, as Car::SetState keeps them).  Arena counters
+ * (tick count, episode ticks) are not rewound, as in the reference.  Call rsb_build_obs
+ * afterwards if observations are needed (CudaEnvSet.cpp:800-806 does). */
+typedef struct rsb_ring_config {
+    int32_t depth;                  /* slots, >= 2 (10); 0 turns the ring off and frees it */
+    int32_t capture_every;          /* env steps between captures in rsb_ring_maybe_capture (3) */
+    float restore_fraction;         /* share of arenas per restore, clamped to [0.01, 0.05] (0.05) */
+    int32_t max_arenas_per_restore; /* cap per restore, also <= 5 % of the arenas (64) */
+    float fuzz_pos;                 /* uu of position jitter (25) */
+    float fuzz_vel;                 /* uu/s of velocity jitter (80) */
+    int32_t lookback_slots;         /* slots back from the newest capture, 1 .. depth-1 (7) */
+    uint32_t seed;                  /* xorshift32 state of the restore draws (0xA5A5A5A5) */
+} rsb_ring_config;
+
+typedef struct rsb_ring_stats {
+    int32_t depth, filled, write_idx, replay_disabled;
+    uint64_t captures, restores, restore_calls;
+} rsb_ring_stats;
+
+/* The reference's defaults (CudaEnvSet.h:100-109, rng CudaEnvSet.h:164). */
+rsb_status rsb_ring_default_config(rsb_ring_config* out);
+/* ConfigureStateRing (CudaEnvSet.cpp:619-656): clamps the fields as the reference does and
+ * allocates depth slots of the batch's car, ball and pad records (2,428 B per 3v3 arena per
+ * slot).  Synchronises the handle's stream. */
+rsb_status rsb_ring_configure(rsb_handle* h, const rsb_ring_config* cfg);
+/* CaptureStateRingSlot (CudaEnvSet.cpp:669-696): the live records into the next slot. */
+rsb_status rsb_ring_capture(rsb_handle* h, void* stream);
+/* MaybeCaptureStateRing (CudaEnvSet.cpp:658-667): counts env steps, captures every
+ * capture_every-th call. */
+rsb_status rsb_ring_maybe_capture(rsb_handle* h, void* stream);
+/* RestoreStateRingReplay (CudaEnvSet.cpp:755-815): negative restore_fraction / lookback_slots
+ * / max_arenas take the configured values; *restored = arenas rewound (0 with fewer than two
+ * captures, with the ring off, or once the reference's tripwire - more than 32 calls and
+ * more than 4 per capture - has turned replay off). */
+rsb_status rsb_ring_restore(rsb_handle* h, float restore_fraction, int32_t lookback_slots, float fuzz_scale,
+                            int32_t max_arenas, int32_t* restored, void* stream);
+rsb_status rsb_ring_stats_get(rsb_handle* h, rsb_ring_stats* out);
+
 /* ---- GAE over a flat rollout buffer (no handle) ----
  * rsb_compute_gae replaces rsc::ComputeGAEOnDevice (RocketSimCuda/include/
  * RocketSimCudaTraining.h:17-30, RocketSimCuda/src/GAECuda.cu:247-300) with the same

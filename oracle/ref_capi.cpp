@@ -76,6 +76,21 @@ struct rsb_handle {
     std::vector<OracleEnv> env;
     std::vector<float> obs, rewardsOut;
     std::vector<uint8_t> masks, terminalsOut;
+    // state ring: CudaEnvSet's host-side ring (CudaEnvSet.h:148-170), slots of public states
+    struct ArenaSnap {
+        std::vector<CarState> cars;
+        BallState ball;
+        std::vector<BoostPadState> pads;
+        bool valid = false;
+    };
+    struct Ring {
+        bool enabled = false, replayDisabled = false;
+        rsb_ring_config cfg{};
+        uint32_t rng = 0xA5A5A5A5u;
+        std::vector<std::vector<ArenaSnap>> slots;
+        int writeIdx = 0, filled = 0, stepsSinceCapture = 0;
+        uint64_t captures = 0, restores = 0, restoreCalls = 0;
+    } ring;
 };
 
 static std::string g_createError;
@@ -484,6 +499,167 @@ rsb_status rsb_culler_set(rsb_handle* h, const float*, float) { return fail(h, R
 rsb_status rsb_culler_distance(rsb_handle* h, const float*, int32_t, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 rsb_status rsb_culler_predict(rsb_handle* h, const float*, int32_t, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 rsb_status rsb_culler_gradients(rsb_handle* h, const float*, const float*, int32_t, float, float*, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
+
+// ---- state ring: CudaEnvSet.cpp:608-815 restated on the RocketSim arenas ----
+
+static float ringRand01(uint32_t& rng) {  // CudaEnvSet.cpp:608-613
+    rng ^= rng << 13;
+    rng ^= rng >> 17;
+    rng ^= rng << 5;
+    return (rng & 0xFFFFFFu) / float(0xFFFFFFu);
+}
+static float ringRange(uint32_t& rng, float lo, float hi) { return lo + (hi - lo) * ringRand01(rng); }
+
+rsb_status rsb_ring_default_config(rsb_ring_config* out) {  // CudaEnvSet.h:100-109, :164
+    if (!out) return RSB_ERR_INVALID;
+    out->depth = 10;
+    out->capture_every = 3;
+    out->restore_fraction = 0.05f;
+    out->max_arenas_per_restore = 64;
+    out->fuzz_pos = 25.f;
+    out->fuzz_vel = 80.f;
+    out->lookback_slots = 7;
+    out->seed = 0xA5A5A5A5u;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_configure(rsb_handle* h, const rsb_ring_config* cfg) {  // ConfigureStateRing :619-656
+    if (!h || !cfg) return fail(h, RSB_ERR_INVALID, "rsb_ring_configure: null argument");
+    auto& R = h->ring;
+    R.slots.clear();
+    R.enabled = false;
+    R.filled = R.writeIdx = R.stepsSinceCapture = 0;
+    const int numArenas = (int)h->arenas.size();
+    if (cfg->depth <= 0 || numArenas <= 0) return RSB_OK;
+    R.cfg = *cfg;
+    const int depth = (std::max)(2, cfg->depth);
+    R.cfg.depth = depth;
+    R.cfg.capture_every = (std::max)(1, cfg->capture_every);
+    R.cfg.lookback_slots = (std::max)(1, (std::min)(cfg->lookback_slots, depth - 1));
+    R.cfg.restore_fraction =
+        (std::max)(0.01f, (std::min)(0.05f, cfg->restore_fraction > 0.f ? cfg->restore_fraction : 0.05f));
+    R.cfg.max_arenas_per_restore = (std::max)(1, cfg->max_arenas_per_restore > 0 ? cfg->max_arenas_per_restore : 64);
+    R.rng = cfg->seed ? cfg->seed : 0xA5A5A5A5u;
+    R.slots.assign((size_t)depth, std::vector<rsb_handle::ArenaSnap>((size_t)numArenas));
+    R.enabled = true;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_capture(rsb_handle* h, void*) {  // CaptureStateRingSlot :669-696
+    if (!h) return RSB_ERR_INVALID;
+    auto& R = h->ring;
+    if (!R.enabled) return RSB_OK;
+    auto& arenas = R.slots[(size_t)R.writeIdx];
+    for (size_t a = 0; a < h->arenas.size(); a++) {
+        auto& snap = arenas[a];
+        snap.cars.clear();
+        for (Car* car : h->cars[a]) snap.cars.push_back(car->GetState());
+        snap.ball = h->arenas[a]->ball->GetState();
+        snap.pads.clear();
+        for (auto* pad : h->arenas[a]->GetBoostPads()) snap.pads.push_back(pad->GetState());
+        snap.valid = true;
+    }
+    R.writeIdx = (R.writeIdx + 1) % R.cfg.depth;
+    if (R.filled < R.cfg.depth) R.filled++;
+    R.captures++;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_maybe_capture(rsb_handle* h, void* stream) {  // MaybeCaptureStateRing :658-667
+    if (!h) return RSB_ERR_INVALID;
+    auto& R = h->ring;
+    if (!R.enabled) return RSB_OK;
+    if (++R.stepsSinceCapture < R.cfg.capture_every) return RSB_OK;
+    R.stepsSinceCapture = 0;
+    return rsb_ring_capture(h, stream);
+}
+
+// ApplyArenaSnap (:698-753): public states of the slot, jittered, through the setters
+static void applyArenaSnap(rsb_handle* h, int a, int slot, float fuzzScale) {
+    auto& R = h->ring;
+    const auto& snap = R.slots[(size_t)slot][(size_t)a];
+    if (!snap.valid) return;
+    const float fp = R.cfg.fuzz_pos * fuzzScale;
+    const float fv = R.cfg.fuzz_vel * fuzzScale;
+    for (size_t c = 0; c < h->cars[a].size() && c < snap.cars.size(); c++) {
+        CarState car = snap.cars[c];
+        if (fp > 0.f) {
+            car.pos.x += ringRange(R.rng, -fp, fp);
+            car.pos.y += ringRange(R.rng, -fp, fp);
+            car.pos.z = (std::max)(17.f, car.pos.z + ringRange(R.rng, -fp * 0.25f, fp * 0.35f));
+        }
+        if (fv > 0.f) {
+            car.vel.x += ringRange(R.rng, -fv, fv);
+            car.vel.y += ringRange(R.rng, -fv, fv);
+            car.vel.z += ringRange(R.rng, -fv * 0.5f, fv * 0.5f);
+        }
+        h->cars[a][c]->SetState(car);
+    }
+    BallState ball = snap.ball;
+    if (fp > 0.f) {
+        ball.pos.x += ringRange(R.rng, -fp, fp);
+        ball.pos.y += ringRange(R.rng, -fp, fp);
+        ball.pos.z = (std::max)(93.f, ball.pos.z + ringRange(R.rng, -fp * 0.2f, fp * 0.4f));
+    }
+    if (fv > 0.f) {
+        ball.vel.x += ringRange(R.rng, -fv, fv);
+        ball.vel.y += ringRange(R.rng, -fv, fv);
+        ball.vel.z += ringRange(R.rng, -fv * 0.5f, fv * 0.5f);
+    }
+    h->arenas[a]->ball->SetState(ball);
+    auto& pads = h->arenas[a]->GetBoostPads();
+    for (size_t p = 0; p < pads.size() && p < snap.pads.size(); p++) pads[p]->SetState(snap.pads[p]);
+}
+
+rsb_status rsb_ring_restore(rsb_handle* h, float restore_fraction, int32_t lookback_slots, float fuzz_scale,
+                            int32_t max_arenas, int32_t* restored, void*) {  // RestoreStateRingReplay :755-815
+    if (!h) return RSB_ERR_INVALID;
+    if (restored) *restored = 0;
+    auto& R = h->ring;
+    if (!R.enabled || R.replayDisabled || R.filled < 2) return RSB_OK;
+    const int numArenas = (int)h->arenas.size();
+    float frac = restore_fraction >= 0.f ? restore_fraction : R.cfg.restore_fraction;
+    frac = (std::max)(0.01f, (std::min)(0.05f, frac));
+    int lookback = lookback_slots >= 0 ? lookback_slots : R.cfg.lookback_slots;
+    lookback = (std::max)(1, (std::min)(lookback, R.filled - 1));
+    int lastWritten = R.writeIdx - 1;
+    if (lastWritten < 0) lastWritten = R.cfg.depth - 1;
+    int slot = lastWritten - lookback;
+    while (slot < 0) slot += R.cfg.depth;
+    int cap = max_arenas > 0 ? max_arenas : R.cfg.max_arenas_per_restore;
+    if (cap <= 0) cap = 64;
+    int fivePct = (std::max)(1, (int)std::lround(0.05 * (double)numArenas));
+    cap = (std::min)(cap, fivePct);
+    int nRestore = (std::max)(1, (int)std::lround(frac * (double)numArenas));
+    nRestore = (std::min)(nRestore, numArenas);
+    nRestore = (std::min)(nRestore, cap);
+    std::vector<int> order((size_t)numArenas);
+    for (int i = 0; i < numArenas; i++) order[(size_t)i] = i;
+    for (int i = 0; i < nRestore; i++) {
+        int j = i + (int)(ringRand01(R.rng) * (numArenas - i));
+        if (j >= numArenas) j = numArenas - 1;
+        std::swap(order[(size_t)i], order[(size_t)j]);
+    }
+    for (int i = 0; i < nRestore; i++) applyArenaSnap(h, order[(size_t)i], slot, fuzz_scale);
+    R.restores += (uint64_t)nRestore;
+    R.restoreCalls++;
+    if (R.restoreCalls > 32 && R.captures > 0 && R.restoreCalls > R.captures * 4) R.replayDisabled = true;
+    if (restored) *restored = nRestore;
+    return RSB_OK;
+}
+
+rsb_status rsb_ring_stats_get(rsb_handle* h, rsb_ring_stats* out) {
+    if (!h || !out) return RSB_ERR_INVALID;
+    const auto& R = h->ring;
+    out->depth = R.enabled ? R.cfg.depth : 0;
+    out->filled = R.filled;
+    out->write_idx = R.writeIdx;
+    out->replay_disabled = R.replayDisabled ? 1 : 0;
+    out->captures = R.captures;
+    out->restores = R.restores;
+    out->restore_calls = R.restoreCalls;
+    return RSB_OK;
+}
 
 // GAE lives in its own oracle libraries (gae_oracle.c, gae_pin.cpp); this one only answers
 // the ABI.

@@ -373,6 +373,36 @@ def run_ours(args, rank, world, dist):
         d2h.append(obs.nbytes + masks.nbytes + rew.nbytes + term.nbytes)
     e2e_value = wl.num_arenas * wl.tick_skip * world / reduce_max(statistics.median(e2e_times), dist, dev)
 
+    # state ring: a device capture (slot copies in HBM) and a restore, against the reference's
+    # capture path (synchronise, download every car, ball and pad state)
+    ring = None
+    if wl.preset == "c3" and not args.no_ring:
+        batch.ring_configure(depth=10, capture_every=1)
+        cap_ms, res_ms = [], []
+        for k in range(6):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            batch.ring_capture(stream=sp)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            cap_ms.append(e0.elapsed_time(e1))
+        for k in range(5):
+            t0 = time.perf_counter()
+            n_rest = batch.ring_restore(stream=sp)
+            torch.cuda.synchronize()
+            res_ms.append(1e3 * (time.perf_counter() - t0))
+        host_ms = []
+        for k in range(3):
+            t0 = time.perf_counter()
+            batch.get_cars(), batch.get_balls(), batch.get_pads()
+            host_ms.append(1e3 * (time.perf_counter() - t0))
+        slot_bytes = (23 + 86 * rsb.RSB_MAX_CARS_PER_ARENA + 2 * rsb.RSB_NUM_PADS) * 4 * wl.num_arenas
+        cms = statistics.median(cap_ms[1:])
+        ring = {"slot_bytes": slot_bytes, "capture_ms": cms, "capture_gbs": 2 * slot_bytes / cms / 1e6,
+                "restore_ms_wall": statistics.median(res_ms), "arenas_per_restore": n_rest,
+                "reference_style_host_capture_ms": statistics.median(host_ms)}
+        batch.ring_configure(depth=0)
+
     # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
     # state read + written per launch (the library reports it), over the kernel's own time
     alg_bytes = batch.stats()["state_bytes_per_step"]
@@ -396,6 +426,7 @@ def run_ours(args, rank, world, dist):
         # per env step: action expansion, (culler,) step, obs + masks, rewards + terminals, reset
         "gpu_launches": steps * (6 if learned is not None else 5),
         "learned_cull": learned,
+        "state_ring": ring,
         "autotune": tune,
         "clocks": clocks[-1],
         "clocks_exact": clocks[0],
@@ -676,6 +707,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gae", action="store_true", help="skip the GAE measurement of the c3 line")
+    ap.add_argument("--no-ring", action="store_true", help="skip the state-ring measurement of the c3 line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

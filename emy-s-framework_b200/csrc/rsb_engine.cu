@@ -1403,4 +1403,43 @@ rsb_status rsb_copy_terminals(rsb_handle* h, uint8_t* out, size_t n) {
     return copyOut(h, out, h ? h->dTerminals : nullptr, n, h ? (size_t)h->N : 0, 1, "terminals");
 }
 
+rsb_status rsb_copy_outputs(rsb_handle* h, float* obs, uint8_t* masks, float* rewards, uint8_t* terminals) {
+    if (!h) return RSB_ERR_INVALID;
+    RSB_CUDA(cudaSetDevice(h->device));
+    if (obs)
+        RSB_CUDA(cudaMemcpyAsync(obs, h->dObs, (size_t)h->numCars * h->obsStride * 4, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    if (masks)
+        RSB_CUDA(cudaMemcpyAsync(masks, h->dMasks, (size_t)h->numCars * RSB_NUM_ACTIONS, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    if (rewards)
+        RSB_CUDA(cudaMemcpyAsync(rewards, h->dRewards, (size_t)h->numCars * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (terminals)
+        RSB_CUDA(cudaMemcpyAsync(terminals, h->dTerminals, (size_t)h->N, cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
+}
+
+rsb_status rsb_host_register(void* ptr, size_t bytes) {
+    if (!ptr || bytes == 0) return RSB_ERR_INVALID;
+    const cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        g_createError = std::string("rsb_host_register: ") + cudaGetErrorString(e);
+        return RSB_ERR_CUDA;
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_host_unregister(void* ptr) {
+    if (!ptr) return RSB_ERR_INVALID;
+    const cudaError_t e = cudaHostUnregister(ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        g_createError = std::string("rsb_host_unregister: ") + cudaGetErrorString(e);
+        return RSB_ERR_CUDA;
+    }
+    return RSB_OK;
+}
+
 }  // extern "C"

@@ -222,6 +222,9 @@ _SIGS = {
     "rsb_get_pads": [_P, _P, C.c_int32],
     "rsb_set_pads": [_P, _P, C.c_int32],
     "rsb_get_arena_info": [_P, _P, C.c_int32],
+    "rsb_copy_outputs": [_P, _P, _P, _P, _P],
+    "rsb_host_register": [_P, C.c_size_t],
+    "rsb_host_unregister": [_P],
     "rsb_ring_default_config": [_P],
     "rsb_ring_configure": [_P, _P],
     "rsb_ring_capture": [_P, _P],
@@ -425,9 +428,44 @@ class Batch:
             raise RsbError(st, self._error(self._h))
 
     def close(self):
+        for a in getattr(self, "_pinned", []):
+            self.lib.rsb_host_unregister(C.c_void_p(a.ctypes.data))
+        self._pinned = []
         if self._h:
             self.lib.rsb_destroy(self._h)
             self._h = C.c_void_p()
+
+    def pin(self, a: np.ndarray) -> np.ndarray:
+        """Page-locks a host array for fast copies (rsb_host_register); it stays registered
+        until the batch is closed."""
+        a = np.ascontiguousarray(a)
+        self._check_global(self.lib.rsb_host_register(C.c_void_p(a.ctypes.data), a.nbytes))
+        if not hasattr(self, "_pinned"):
+            self._pinned = []
+        self._pinned.append(a)
+        return a
+
+    def pinned_outputs(self) -> dict:
+        """Page-locked host arrays for the observation rows, masks, rewards and terminals,
+        allocated once; copy_outputs() fills them in place every step."""
+        return {"obs": self.pin(np.zeros((self.num_cars, self.obs_stride), np.float32)),
+                "masks": self.pin(np.zeros((self.num_cars, RSB_NUM_ACTIONS), np.uint8)),
+                "rewards": self.pin(np.zeros(max(1, self.num_cars), np.float32)),
+                "terminals": self.pin(np.zeros(self.num_arenas, np.uint8))}
+
+    def copy_outputs(self, bufs: dict) -> dict:
+        """rsb_copy_outputs: the four output buffers into `bufs` (see pinned_outputs), one
+        synchronisation."""
+        p = {k: (C.c_void_p(bufs[k].ctypes.data) if k in bufs else None)
+             for k in ("obs", "masks", "rewards", "terminals")}
+        if "obs" in bufs:
+            assert bufs["obs"].size == self.num_cars * self.obs_stride
+        self._check(self.lib.rsb_copy_outputs(self._h, p["obs"], p["masks"], p["rewards"], p["terminals"]))
+        return bufs
+
+    def _check_global(self, st: int):
+        if st != 0:
+            raise RsbError(st, _global_error(self.lib))
 
     def __del__(self):
         try:

@@ -367,6 +367,18 @@ rsb_status rsb_culler_predict(rsb_handle* h, const float* pts, int32_t n, float*
 rsb_status rsb_culler_gradients(rsb_handle* h, const float* pts, const float* target, int32_t n,
                                 float over_weight, float* grad, float* loss);
 
+/* The four CopyBuilt* calls of CudaEnvSet.cpp:163-166 in one: the observation rows, masks,
+ * rewards and terminals queued on the handle's stream, then one synchronisation.  A NULL
+ * destination is skipped.  Sizes are those of rsb_copy_obs / _masks / _rewards / _terminals. */
+rsb_status rsb_copy_outputs(rsb_handle* h, float* obs, uint8_t* masks, float* rewards, uint8_t* terminals);
+
+/* Page-locks (and releases) a caller's host buffer, so that the copies to and from it run at
+ * full PCIe speed without staging (cudaHostRegister, portable to every device).  No
+ * counterpart in the reference, whose host vectors are pageable.  Register a buffer once,
+ * reuse it every step, and unregister it before freeing it. */
+rsb_status rsb_host_register(void* ptr, size_t bytes);
+rsb_status rsb_host_unregister(void* ptr);
+
 /* ---- state ring: rewind a few arenas to an earlier state ----
  * Replaces the state ring of GGL::CudaEnvSet (GigaLearnCPP/src/public/GigaLearnCPP/Sim/
  * CudaEnvSet.h:100-125, CudaEnvSet.cpp:608-815).  The reference copies every car, ball and

@@ -500,6 +500,19 @@ rsb_status rsb_culler_distance(rsb_handle* h, const float*, int32_t, float*) { r
 rsb_status rsb_culler_predict(rsb_handle* h, const float*, int32_t, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 rsb_status rsb_culler_gradients(rsb_handle* h, const float*, const float*, int32_t, float, float*, float*) { return fail(h, RSB_ERR_UNSUPPORTED, "no culler on the CPU oracle"); }
 
+rsb_status rsb_copy_outputs(rsb_handle* h, float* obs, uint8_t* masks, float* rewards, uint8_t* terminals) {
+    if (!h) return RSB_ERR_INVALID;
+    rsb_status st = RSB_OK;
+    if (obs && st == RSB_OK) st = rsb_copy_obs(h, obs, h->obs.size());
+    if (masks && st == RSB_OK) st = rsb_copy_masks(h, masks, h->masks.size());
+    if (rewards && st == RSB_OK) st = rsb_copy_rewards(h, rewards, h->rewardsOut.size());
+    if (terminals && st == RSB_OK) st = rsb_copy_terminals(h, terminals, h->terminalsOut.size());
+    return st;
+}
+// host memory needs no pinning on the CPU oracle
+rsb_status rsb_host_register(void* ptr, size_t bytes) { return ptr && bytes ? RSB_OK : RSB_ERR_INVALID; }
+rsb_status rsb_host_unregister(void* ptr) { return ptr ? RSB_OK : RSB_ERR_INVALID; }
+
 // ---- state ring: CudaEnvSet.cpp:608-815 restated on the RocketSim arenas ----
 
 static float ringRand01(uint32_t& rng) {  // CudaEnvSet.cpp:608-613

@@ -410,6 +410,10 @@ def run_ours(args, rank, world, dist):
     # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
     # state read + written per launch (the library reports it), over the kernel's own time
     alg_bytes = batch.stats()["state_bytes_per_step"]
+    # DRAM traffic of a settled 3v3 step-kernel launch, measured by ncu on 8,192 arenas
+    # (dram__bytes_read.sum + dram__bytes_write.sum = 58,409 B per arena, the threads' local
+    # memory), scaled by the arenas; no capture exists for other team sizes
+    traffic = 58409 * wl.num_arenas if (wl.team_size == 3 and not wl.mixed) else None
     kernel_s = statistics.mean(step_times) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / kernel_s / 1e9
@@ -422,7 +426,9 @@ def run_ours(args, rank, world, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random states)",
         "config": cfg,
         "roofline": {"bound": "hbm", "kernel": "stepKernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic_source": "ncu dram bytes of a settled 3v3 x 8192 launch, scaled by arenas"
+                     if traffic else None,
                      "bytes_per_launch": alg_bytes, "kernel_ms": kernel_s * 1e3,
                      "kernel_share": statistics.mean(step_times) / (total_ms / steps)},
         "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": int(statistics.mean(h2d)),
@@ -607,7 +613,9 @@ def run_gae(args, rank, world, dist, steps, warmup, reference_device=False):
     achieved = alg_bytes / (ms / 1e3) / 1e9
     res = {"value": T * world / (ms / 1e3), "unit": "elements/s", "ms_per_call": ms, "elements": T,
            "roofline": {"bound": "hbm", "kernel": "gaeSegmentKernel (+ summary and scan)", "achieved": achieved,
-                        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                        "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        # ncu dram__bytes_read.sum + write.sum of gaeSegmentKernel on this buffer
+                        "traffic": 213854464 if T == GAE_PLAYERS * GAE_STEPS else None,
                         "peak_kind": peak_kind, "bytes_per_call": alg_bytes},
            "gpu_launches": 3 * steps, "clocks": cs.summary()}
     if not reference_device:

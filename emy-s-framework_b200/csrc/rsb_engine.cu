@@ -125,6 +125,8 @@ struct rsb_handle {
     // launch configuration of the step kernel (indices into kStepVariants / kStepBlocks)
     int stepVariant = 0, stepBlock = 1;
     uint32_t* dScratch = nullptr;   // the autotuner's copy of the arena records
+    uint32_t* dStage = nullptr;     // staging of the per-arena getters
+    size_t stageWords = 0;
     EnvTables tables{};
     bool hasRewards = false;
     RewardParams rewardParams{};
@@ -248,6 +250,51 @@ __global__ void ringRestoreKernel(uint32_t* ball, uint32_t* car, uint32_t* pad, 
         pp.bits = (pp.bits & 1u) | ((pp.bits >> 8) << 8);  // is_active and prev_locked_car_id
         storePlanes(pp, pad, p * N + a, N * NUM_PADS);
     }
+}
+
+// Single-record access for the per-arena getters and setters: gathers `count` records of
+// `words` words (record r at base + r * recStep, word stride `stride`) into out[r * words + w].
+__global__ void gatherRecordsKernel(const uint32_t* planes, int base, int recStep, int count, int stride, int words,
+                                    uint32_t* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count * words) return;
+    const int r = i / words, w = i % words;
+    out[i] = planes[(size_t)w * stride + base + (size_t)r * recStep];
+}
+
+// Car::SetState on one car record (the host setter's conversion, on the device).
+__global__ void setCarKernel(uint32_t* car, int idx, int stride, rsb_car_state s) {
+    CarP p;
+    loadPlanes(p, car, idx, stride);
+    applyCarState(p, s);
+    storePlanes(p, car, idx, stride);
+}
+
+// Ball::SetState on one arena's ball, with the goal-line flag kept in step (as rsb_set_balls).
+__global__ void setBallKernel(uint32_t* ball, uint32_t* arena, int a, int N, rsb_ball_state s, float goalLine) {
+    BallP p;
+    loadPlanes(p, ball, a, N);
+    applyBallState(p, s);
+    storePlanes(p, ball, a, N);
+    ArenaP ap;
+    loadPlanes(ap, arena, a, N);
+    const float y = p.pos[1] * kBtToUu;
+    ap.scored = fabsf(y) > goalLine ? (p.pos[1] > 0 ? 1 : 2) : 0;
+    storePlanes(ap, arena, a, N);
+}
+
+struct PadSet {
+    rsb_pad_state p[NUM_PADS];
+};
+
+// BoostPad::SetState on the 34 pads of one arena.
+__global__ void setPadsKernel(uint32_t* pad, int a, int N, PadSet s) {
+    const int p = threadIdx.x;
+    if (p >= NUM_PADS) return;
+    PadP pp;
+    pp.cooldown = s.p[p].cooldown;
+    pp.bits = (s.p[p].is_active ? 1u : 0u) | (s.p[p].prev_locked_car_id << 8);
+    storePlanes(pp, pad, p * N + a, N * NUM_PADS);
 }
 
 __global__ void expandActionsKernel(const int32_t* idx, const rsb_controls* lut, int lutCount, rsb_controls* out, int n) {
@@ -502,7 +549,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
     cudaFree(h->dTris);
     cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
-    cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs);
+    cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return RSB_OK;
@@ -771,6 +818,18 @@ rsb_status rsb_set_pads(rsb_handle* h, const rsb_pad_state* in, int32_t n) {
     return upload(h, h->dPad, planes);
 }
 
+static rsb_arena_info arenaInfoOf(const ArenaP& ap, int teamSize) {
+    rsb_arena_info o{};
+    o.tick_count = (uint64_t)ap.tick[0] | ((uint64_t)ap.tick[1] << 32);
+    o.num_cars = 2 * teamSize;
+    o.team_size = teamSize;
+    o.goal_scored = ap.scored != 0;
+    o.goal_team = ap.scored == 1 ? 0 : (ap.scored == 2 ? 1 : -1);
+    o.episode_ticks = ap.episodeTicks;
+    o.status = ap.status;
+    return o;
+}
+
 rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
     if (!h || !out || n != h->N) return fail(h, RSB_ERR_INVALID, "info count must equal num_arenas");
     std::vector<uint32_t> planes;
@@ -779,16 +838,111 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
     for (int a = 0; a < n; a++) {
         ArenaP ap;
         loadPlanes(ap, planes.data(), a, h->N);
-        rsb_arena_info& o = out[a];
-        o = rsb_arena_info{};
-        o.tick_count = (uint64_t)ap.tick[0] | ((uint64_t)ap.tick[1] << 32);
-        o.num_cars = 2 * h->teamSize[a];
-        o.team_size = h->teamSize[a];
-        o.goal_scored = ap.scored != 0;
-        o.goal_team = ap.scored == 1 ? 0 : (ap.scored == 2 ? 1 : -1);
-        o.episode_ticks = ap.episodeTicks;
-        o.status = ap.status;
+        out[a] = arenaInfoOf(ap, h->teamSize[a]);
     }
+    return RSB_OK;
+}
+
+// ---- one arena at a time (RocketSimCuda.h:349-378): a gather kernel and one small copy, or
+// one small kernel, instead of a whole-batch transfer ----
+
+static rsb_status gatherRecords(rsb_handle* h, const uint32_t* planes, int base, int recStep, int count, int stride,
+                                int words, std::vector<uint32_t>& out) {
+    RSB_CUDA(cudaSetDevice(h->device));
+    const size_t need = (size_t)count * words;
+    if (h->stageWords < need) {
+        cudaFree(h->dStage);
+        h->dStage = nullptr;
+        h->stageWords = 0;
+        RSB_CUDA(cudaMalloc(&h->dStage, need * 4));
+        h->stageWords = need;
+    }
+    gatherRecordsKernel<<<(unsigned)((need + 127) / 128), 128, 0, h->stream>>>(planes, base, recStep, count, stride,
+                                                                                 words, h->dStage);
+    RSB_CUDA(cudaGetLastError());
+    out.resize(need);
+    RSB_CUDA(cudaMemcpyAsync(out.data(), h->dStage, need * 4, cudaMemcpyDeviceToHost, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
+}
+
+static bool carIndex(const rsb_handle* h, int32_t arena, int32_t car) {
+    return arena >= 0 && arena < h->N && car >= 0 && car < 2 * h->teamSize[arena];
+}
+
+rsb_status rsb_get_car_at(rsb_handle* h, int32_t arena, int32_t car, rsb_car_state* out) {
+    if (!h || !out || !carIndex(h, arena, car)) return fail(h, RSB_ERR_INVALID, "rsb_get_car_at: no such car");
+    std::vector<uint32_t> w;
+    rsb_status st = gatherRecords(h, h->dCar, car * h->N + arena, 0, 1, MAX_CARS * h->N, W_CAR, w);
+    if (st) return st;
+    CarP p;
+    loadPlanes(p, w.data(), 0, 1);
+    *out = carStateOf(p, (uint32_t)car + 1u);
+    return RSB_OK;
+}
+
+rsb_status rsb_set_car_at(rsb_handle* h, int32_t arena, int32_t car, const rsb_car_state* in) {
+    if (!h || !in || !carIndex(h, arena, car)) return fail(h, RSB_ERR_INVALID, "rsb_set_car_at: no such car");
+    RSB_CUDA(cudaSetDevice(h->device));
+    setCarKernel<<<1, 1, 0, h->stream>>>(h->dCar, car * h->N + arena, MAX_CARS * h->N, *in);
+    RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+rsb_status rsb_get_ball_at(rsb_handle* h, int32_t arena, rsb_ball_state* out) {
+    if (!h || !out || arena < 0 || arena >= h->N) return fail(h, RSB_ERR_INVALID, "rsb_get_ball_at: no such arena");
+    std::vector<uint32_t> w;
+    rsb_status st = gatherRecords(h, h->dBall, arena, 0, 1, h->N, W_BALL, w);
+    if (st) return st;
+    BallP p;
+    loadPlanes(p, w.data(), 0, 1);
+    *out = ballStateOf(p);
+    return RSB_OK;
+}
+
+rsb_status rsb_set_ball_at(rsb_handle* h, int32_t arena, const rsb_ball_state* in) {
+    if (!h || !in || arena < 0 || arena >= h->N) return fail(h, RSB_ERR_INVALID, "rsb_set_ball_at: no such arena");
+    RSB_CUDA(cudaSetDevice(h->device));
+    setBallKernel<<<1, 1, 0, h->stream>>>(h->dBall, h->dArena, arena, h->N, *in, h->P.goalBaseY + h->P.ballRadiusUu);
+    RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+rsb_status rsb_get_pads_at(rsb_handle* h, int32_t arena, rsb_pad_state* out) {
+    if (!h || !out || arena < 0 || arena >= h->N) return fail(h, RSB_ERR_INVALID, "rsb_get_pads_at: no such arena");
+    std::vector<uint32_t> w;
+    rsb_status st = gatherRecords(h, h->dPad, arena, h->N, NUM_PADS, h->N * NUM_PADS, W_PAD, w);
+    if (st) return st;
+    for (int p = 0; p < NUM_PADS; p++) {
+        PadP pp;
+        loadPlanes(pp, w.data() + (size_t)p * W_PAD, 0, 1);
+        out[p] = rsb_pad_state{};
+        out[p].is_active = pp.bits & 1;
+        out[p].cooldown = pp.cooldown;
+        out[p].prev_locked_car_id = pp.bits >> 8;
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_set_pads_at(rsb_handle* h, int32_t arena, const rsb_pad_state* in) {
+    if (!h || !in || arena < 0 || arena >= h->N) return fail(h, RSB_ERR_INVALID, "rsb_set_pads_at: no such arena");
+    RSB_CUDA(cudaSetDevice(h->device));
+    PadSet ps;
+    std::memcpy(ps.p, in, sizeof ps.p);
+    setPadsKernel<<<1, 64, 0, h->stream>>>(h->dPad, arena, h->N, ps);
+    RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+rsb_status rsb_get_arena_info_at(rsb_handle* h, int32_t arena, rsb_arena_info* out) {
+    if (!h || !out || arena < 0 || arena >= h->N)
+        return fail(h, RSB_ERR_INVALID, "rsb_get_arena_info_at: no such arena");
+    std::vector<uint32_t> w;
+    rsb_status st = gatherRecords(h, h->dArena, arena, 0, 1, h->N, W_ARENA, w);
+    if (st) return st;
+    ArenaP ap;
+    loadPlanes(ap, w.data(), 0, 1);
+    *out = arenaInfoOf(ap, h->teamSize[arena]);
     return RSB_OK;
 }
 

@@ -223,6 +223,13 @@ _SIGS = {
     "rsb_set_pads": [_P, _P, C.c_int32],
     "rsb_get_arena_info": [_P, _P, C.c_int32],
     "rsb_copy_outputs": [_P, _P, _P, _P, _P],
+    "rsb_get_car_at": [_P, C.c_int32, C.c_int32, _P],
+    "rsb_set_car_at": [_P, C.c_int32, C.c_int32, _P],
+    "rsb_get_ball_at": [_P, C.c_int32, _P],
+    "rsb_set_ball_at": [_P, C.c_int32, _P],
+    "rsb_get_pads_at": [_P, C.c_int32, _P],
+    "rsb_set_pads_at": [_P, C.c_int32, _P],
+    "rsb_get_arena_info_at": [_P, C.c_int32, _P],
     "rsb_host_register": [_P, C.c_size_t],
     "rsb_host_unregister": [_P],
     "rsb_ring_default_config": [_P],
@@ -574,6 +581,40 @@ class Batch:
         self._check(self.lib.rsb_culler_gradients(self._h, _ptr(p), _ptr(t), len(p), over_weight, _ptr(g),
                                                   C.byref(loss)))
         return g, loss.value
+
+    # ---------------------------------------------------------------- one arena
+    def get_car(self, arena: int, car: int) -> np.ndarray:
+        out = np.zeros(1, CAR_DTYPE)
+        self._check(self.lib.rsb_get_car_at(self._h, arena, car, _ptr(out)))
+        return out[0]
+
+    def set_car(self, arena: int, car: int, state):
+        a = np.ascontiguousarray(np.asarray(state, CAR_DTYPE).reshape(1))
+        self._check(self.lib.rsb_set_car_at(self._h, arena, car, _ptr(a)))
+
+    def get_ball(self, arena: int) -> np.ndarray:
+        out = np.zeros(1, BALL_DTYPE)
+        self._check(self.lib.rsb_get_ball_at(self._h, arena, _ptr(out)))
+        return out[0]
+
+    def set_ball(self, arena: int, state):
+        a = np.ascontiguousarray(np.asarray(state, BALL_DTYPE).reshape(1))
+        self._check(self.lib.rsb_set_ball_at(self._h, arena, _ptr(a)))
+
+    def get_arena_pads(self, arena: int) -> np.ndarray:
+        out = np.zeros(RSB_NUM_PADS, PAD_DTYPE)
+        self._check(self.lib.rsb_get_pads_at(self._h, arena, _ptr(out)))
+        return out
+
+    def set_arena_pads(self, arena: int, pads):
+        a = np.ascontiguousarray(np.asarray(pads, PAD_DTYPE))
+        assert a.size == RSB_NUM_PADS
+        self._check(self.lib.rsb_set_pads_at(self._h, arena, _ptr(a)))
+
+    def get_arena_info_at(self, arena: int) -> np.ndarray:
+        out = np.zeros(1, INFO_DTYPE)
+        self._check(self.lib.rsb_get_arena_info_at(self._h, arena, _ptr(out)))
+        return out[0]
 
     # ---------------------------------------------------------------- state ring
     def ring_configure(self, **overrides) -> RingConfig:

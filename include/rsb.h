@@ -302,6 +302,20 @@ rsb_status rsb_get_pads(rsb_handle* h, rsb_pad_state* out, int32_t n);   /* n = 
 rsb_status rsb_set_pads(rsb_handle* h, const rsb_pad_state* in, int32_t n);
 rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n);
 
+/* One arena at a time (RocketSimCudaBatch::GetCarState / GetBallState / GetBoostPadStates /
+ * GetArenaInfo / SetCarState / SetBallState / SetBoostPadStates, RocketSimCuda.h:349-378):
+ * car is the slot within the arena (blue first), pads are 34 records in arena order.  The
+ * getters gather the one record on the device and copy it (synchronising the handle's
+ * stream); the setters launch one small kernel on the handle's stream with the same
+ * conversion as the whole-batch setters, so other arenas are not touched. */
+rsb_status rsb_get_car_at(rsb_handle* h, int32_t arena, int32_t car, rsb_car_state* out);
+rsb_status rsb_set_car_at(rsb_handle* h, int32_t arena, int32_t car, const rsb_car_state* in);
+rsb_status rsb_get_ball_at(rsb_handle* h, int32_t arena, rsb_ball_state* out);
+rsb_status rsb_set_ball_at(rsb_handle* h, int32_t arena, const rsb_ball_state* in);
+rsb_status rsb_get_pads_at(rsb_handle* h, int32_t arena, rsb_pad_state* out);
+rsb_status rsb_set_pads_at(rsb_handle* h, int32_t arena, const rsb_pad_state* in);
+rsb_status rsb_get_arena_info_at(rsb_handle* h, int32_t arena, rsb_arena_info* out);
+
 /* One candidate launch configuration of the step kernel and its measured time. */
 typedef struct rsb_tune_entry {
     int32_t min_blocks;   /* register budget: at least this many 128-thread blocks per SM */

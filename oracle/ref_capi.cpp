@@ -488,6 +488,73 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n) {
     return RSB_OK;
 }
 
+// One arena at a time (RocketSimCuda.h:349-378) on the RocketSim objects.
+static bool validArena(const rsb_handle* h, int32_t a) { return h && a >= 0 && a < (int32_t)h->arenas.size(); }
+
+rsb_status rsb_get_car_at(rsb_handle* h, int32_t a, int32_t c, rsb_car_state* out) {
+    if (!validArena(h, a) || !out || c < 0 || c >= (int32_t)h->cars[a].size()) return fail(h, RSB_ERR_INVALID, "no such car");
+    Car* car = h->cars[a][c];
+    *out = fromCarState(car->GetState(), car->team, car->id);
+    return RSB_OK;
+}
+rsb_status rsb_set_car_at(rsb_handle* h, int32_t a, int32_t c, const rsb_car_state* in) {
+    if (!validArena(h, a) || !in || c < 0 || c >= (int32_t)h->cars[a].size()) return fail(h, RSB_ERR_INVALID, "no such car");
+    h->cars[a][c]->SetState(toCarState(*in));
+    return RSB_OK;
+}
+rsb_status rsb_get_ball_at(rsb_handle* h, int32_t a, rsb_ball_state* out) {
+    if (!validArena(h, a) || !out) return fail(h, RSB_ERR_INVALID, "no such arena");
+    BallState s = h->arenas[a]->ball->GetState();
+    out->pos = fromVec(s.pos);
+    out->rot.forward = fromVec(s.rotMat.forward);
+    out->rot.right = fromVec(s.rotMat.right);
+    out->rot.up = fromVec(s.rotMat.up);
+    out->vel = fromVec(s.vel);
+    out->ang_vel = fromVec(s.angVel);
+    return RSB_OK;
+}
+rsb_status rsb_set_ball_at(rsb_handle* h, int32_t a, const rsb_ball_state* in) {
+    if (!validArena(h, a) || !in) return fail(h, RSB_ERR_INVALID, "no such arena");
+    BallState s;
+    s.pos = toVec(in->pos);
+    s.rotMat = RotMat(toVec(in->rot.forward), toVec(in->rot.right), toVec(in->rot.up));
+    s.vel = toVec(in->vel);
+    s.angVel = toVec(in->ang_vel);
+    h->arenas[a]->ball->SetState(s);
+    return RSB_OK;
+}
+rsb_status rsb_get_pads_at(rsb_handle* h, int32_t a, rsb_pad_state* out) {
+    if (!validArena(h, a) || !out) return fail(h, RSB_ERR_INVALID, "no such arena");
+    auto& pads = h->arenas[a]->GetBoostPads();
+    for (int p = 0; p < RSB_NUM_PADS; p++) {
+        BoostPadState s = pads[p]->GetState();
+        out[p] = rsb_pad_state{};
+        out[p].is_active = s.isActive;
+        out[p].cooldown = s.cooldown;
+        out[p].prev_locked_car_id = s.prevLockedCarID;
+    }
+    return RSB_OK;
+}
+rsb_status rsb_set_pads_at(rsb_handle* h, int32_t a, const rsb_pad_state* in) {
+    if (!validArena(h, a) || !in) return fail(h, RSB_ERR_INVALID, "no such arena");
+    auto& pads = h->arenas[a]->GetBoostPads();
+    for (int p = 0; p < RSB_NUM_PADS; p++) {
+        BoostPadState s;
+        s.isActive = in[p].is_active;
+        s.cooldown = in[p].cooldown;
+        s.prevLockedCarID = in[p].prev_locked_car_id;
+        pads[p]->SetState(s);
+    }
+    return RSB_OK;
+}
+rsb_status rsb_get_arena_info_at(rsb_handle* h, int32_t a, rsb_arena_info* out) {
+    if (!validArena(h, a) || !out) return fail(h, RSB_ERR_INVALID, "no such arena");
+    std::vector<rsb_arena_info> all(h->arenas.size());
+    rsb_status st = rsb_get_arena_info(h, all.data(), (int32_t)all.size());
+    if (st == RSB_OK) *out = all[(size_t)a];
+    return st;
+}
+
 rsb_status rsb_sync(rsb_handle* h) { return h ? RSB_OK : RSB_ERR_INVALID; }
 
 // The learned culler is a GPU component with no CPU counterpart in the reference.

@@ -59,7 +59,11 @@ inline void computeParams(const rsb_mutators& m, WorldParams& P) {
         V3 center = (mn + mx) * 0.5f;
         C.cbt = (radius + length(center)) * 0.02f;
     }
-    const float mass = m.car_mass;
+    // RocketSim builds every car with RLConst::CAR_MASS_BT (Car::_BulletSetup, Car.cpp:206-209):
+    // MutatorConfig::carMass set before the cars exist never reaches them, and the reference
+    // batch simulator uses its constant car mass throughout (CarPhysics.cuh:48, Collision.cuh:506)
+    const float mass = CAR_MASS_BT;
+    (void)m.car_mass;
     C.invMass = 1.f / mass;
     C.mass = 1.f / C.invMass;
     {
@@ -407,7 +411,7 @@ RSB_HD void applyCarState(CarP& p, const rsb_car_state& s) {
     p.worldContactNormal[1] = s.world_contact_normal.y;
     p.worldContactNormal[2] = s.world_contact_normal.z;
     p.carContactOtherId = s.car_contact_other_id;
-    uint32_t f = p.flags & CF_TEAM_ORANGE;
+    uint32_t f = p.flags & (CF_TEAM_ORANGE | CF_NO_RESPONSE);
     if (s.is_on_ground) f |= CF_ON_GROUND;
     if (s.has_jumped) f |= CF_HAS_JUMPED;
     if (s.has_double_jumped) f |= CF_HAS_DOUBLE_JUMPED;

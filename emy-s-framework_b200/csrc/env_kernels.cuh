@@ -406,7 +406,8 @@ RSB_D void putCarF(const EnvView& E, int a, int s, int w, float v) { putCarW(E, 
 // Car.h:15-100): the transform, the velocities and every CarState field are replaced;
 // the broadphase registration and the vehicle's wheel values are kept.
 RSB_D void resetCar(const EnvView& E, int a, int s, V3 posUu, const M3& rot, V3 velUu, V3 ang, float boost) {
-    const uint32_t team = carW(E, a, s, CW_FLAGS) & CF_TEAM_ORANGE;
+    // the team and the body's contact-response flag survive Car::SetState
+    const uint32_t team = carW(E, a, s, CW_FLAGS) & (CF_TEAM_ORANGE | CF_NO_RESPONSE);
     const V3 p = posUu * kUuToBt, v = velUu * kUuToBt;
     const float pv[3] = {p.x, p.y, p.z}, vv[3] = {v.x, v.y, v.z}, av[3] = {ang.x, ang.y, ang.z};
     for (int k = 0; k < 3; k++) {

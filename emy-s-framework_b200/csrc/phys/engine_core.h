@@ -86,6 +86,7 @@ RSB_HD void loadCar(const EngineView& D, int a, int s, Body& b, CarSim& c) {
     b.lin = v3of(p.lin);
     b.ang = v3of(p.ang);
     initBodyCommon(b);
+    b.noResp = (p.flags & CF_NO_RESPONSE) ? 1 : 0;
     b.invMass = C.invMass;
     b.grav = C.grav;
     b.invIl = C.invInertiaLocal;
@@ -166,7 +167,7 @@ RSB_HD void storeCar(const EngineView& D, int a, int s, const Body& b, const Car
     putV3(p.flipRelTorque, c.flipRelTorque);
     putV3(p.worldContactNormal, c.worldContactNormal);
     p.carContactOtherId = c.carContactOtherId;
-    p.flags = c.flags;
+    p.flags = (c.flags & ~CF_NO_RESPONSE) | (b.noResp ? CF_NO_RESPONSE : 0u);
     p.ballHitTick[0] = (uint32_t)c.ballHitTick;
     p.ballHitTick[1] = (uint32_t)(c.ballHitTick >> 32);
     p.ballHitExtraTick[0] = (uint32_t)c.ballHitExtraTick;

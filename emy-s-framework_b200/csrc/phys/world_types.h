@@ -188,7 +188,13 @@ enum : uint32_t {
     CF_SUPERSONIC = 1u << 6, CF_AUTO_FLIPPING = 1u << 7, CF_DEMOED = 1u << 8,
     CF_WORLD_CONTACT = 1u << 9, CF_BALL_HIT_VALID = 1u << 10,
     CF_WHEEL0 = 1u << 11,  // 4 bits: wheelsWithContact
-    CF_TEAM_ORANGE = 1u << 15
+    CF_TEAM_ORANGE = 1u << 15,
+    // btCollisionObject::CF_NO_CONTACT_RESPONSE of the car's rigid body: set by the pre-tick of
+    // a demoed car, cleared by the pre-tick of a live one (Car.cpp:67-83).  It belongs to the
+    // body, so it outlasts the tick (a car that pre-ticks earlier casts its wheel rays past a
+    // demoed car, btDefaultVehicleRaycaster.cpp:43) and Car::SetState leaves it alone.  Not
+    // part of the public CarState.
+    CF_NO_RESPONSE = 1u << 16
 };
 
 }  // namespace rsb

@@ -182,7 +182,9 @@ enum {
 /* RocketSim MutatorConfig (Sim/MutatorConfig/MutatorConfig.h:16-70), soccar defaults when NULL. */
 typedef struct rsb_mutators {
     rsb_vec3 gravity;
-    float car_mass, car_world_friction, car_world_restitution;
+    float car_mass;            /* accepted and ignored, as in the reference: cars keep RocketSim's
+                                  CAR_MASS_BT (Car.cpp:206-209; the batch simulator's CAR_MASS) */
+    float car_world_friction, car_world_restitution;
     float ball_mass, ball_max_speed, ball_drag, ball_world_friction, ball_world_restitution;
     float jump_accel, jump_immediate_force;
     float boost_accel_ground, boost_accel_air, boost_used_per_second;

@@ -27,6 +27,7 @@ struct EngineView {
     const uint32_t* cull;          // per-arena body bits from the learned culler, or null
     int32_t cullAudit;             // run culled static tests anyway and count what they find
     unsigned long long* counters;  // [static tests run, tests culled, culled tests that hit, solver rows], or null
+    unsigned int* work;            // next unclaimed arena of a persistent launch (zeroed before it)
 };
 
 RSB_HD void initBodyCommon(Body& b) {

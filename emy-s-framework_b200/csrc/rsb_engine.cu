@@ -125,6 +125,8 @@ struct rsb_handle {
     // launch configuration of the step kernel (indices into kStepVariants / kStepBlocks)
     int stepVariant = 0, stepBlock = 1;
     uint32_t* dScratch = nullptr;   // the autotuner's copy of the arena records
+    unsigned int* dWork = nullptr;  // claim counter of the persistent step kernel
+    int persistGrid[8][4] = {};     // resident blocks (all SMs) per persistent variant and block size
     uint32_t* dStage = nullptr;     // staging of the per-arena getters
     size_t stageWords = 0;
     EnvTables tables{};
@@ -171,11 +173,37 @@ __global__ void __launch_bounds__(128, MINB) stepKernel(EngineView D, int ticks)
     stepArena(D, a, ticks, A);
 }
 
+// Persistent form: the grid holds only as many blocks as fit on the GPU at once, and each warp
+// claims the next 32 arenas from a counter until none are left.  One arena per thread still,
+// and the same per-arena computation; the claims pack the work that one-arena-per-thread
+// blocks leave in a partial last wave (65,536 arenas are about 1.7 waves of resident warps).
+// No waiting: a claim is one atomic add.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) stepKernelPersistent(EngineView D, int ticks) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = (int)atomicAdd(D.work, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= D.N) return;
+        const int a = base + lane;
+        if (a < D.N) {
+            ArenaSim A;
+            EpaWork epa;
+            A.W.epa = &epa;
+            stepArena(D, a, ticks, A);
+        }
+    }
+}
+
 struct StepVariant {
     void (*fn)(EngineView, int);
     int minBlocks;
+    bool persistent;
 };
-static const StepVariant kStepVariants[] = {{stepKernel<1>, 1}, {stepKernel<3>, 3}, {stepKernel<4>, 4}};
+static const StepVariant kStepVariants[] = {{stepKernel<1>, 1, false},          {stepKernel<3>, 3, false},
+                                            {stepKernel<4>, 4, false},          {stepKernelPersistent<1>, 1, true},
+                                            {stepKernelPersistent<3>, 3, true}, {stepKernelPersistent<4>, 4, true}};
 constexpr int kNumStepVariants = sizeof(kStepVariants) / sizeof(kStepVariants[0]);
 static const int kStepBlocks[] = {32, 64, 128};
 constexpr int kNumStepBlocks = sizeof(kStepBlocks) / sizeof(kStepBlocks[0]);
@@ -335,6 +363,7 @@ static EngineView devView(rsb_handle* h) {
     D.cull = nullptr;
     D.cullAudit = h->cullMode == RSB_CULL_LEARNED_AUDIT;
     D.counters = h->dCounters;
+    D.work = h->dWork;
     return D;
 }
 
@@ -522,7 +551,7 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
         !dalloc(h->dMasks, (size_t)h->numCars * RSB_NUM_ACTIONS) ||
         !dalloc(h->dRewards, (size_t)h->numCars * 4) || !dalloc(h->dTerminals, N) ||
         !dalloc(h->dResetIdx, N * 4) || !dalloc(h->dCull, N * 4) ||
-        !dalloc(h->dCounters, 4 * sizeof(unsigned long long)))
+        !dalloc(h->dCounters, 4 * sizeof(unsigned long long)) || !dalloc(h->dWork, sizeof(unsigned int)))
         return fail(nullptr, RSB_ERR_NOMEM, "device allocation failed");
     cudaMemcpy(h->dTeamSize, h->teamSize.data(), N * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(h->dCarOffset, h->carOffset.data(), (N + 1) * 4, cudaMemcpyHostToDevice);
@@ -549,7 +578,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
     cudaFree(h->dTris);
     cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
-    cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage);
+    cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage); cudaFree(h->dWork);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return RSB_OK;
@@ -571,6 +600,29 @@ rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride) {
     return RSB_OK;
 }
 
+// Launches step-kernel variant v with block size index b on stream st (a persistent variant
+// first zeroes its claim counter on the same stream).
+static cudaError_t launchStep(rsb_handle* h, const EngineView& D, int v, int b, int ticks, cudaStream_t st) {
+    const StepVariant& sv = kStepVariants[v];
+    const int block = kStepBlocks[b];
+    int grid = (h->N + block - 1) / block;
+    if (sv.persistent) {
+        int& g = h->persistGrid[v][b];
+        if (g == 0) {
+            int perSm = 0, sms = 0;
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sv.fn, block, 0);
+            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+            if (e != cudaSuccess) return e;
+            g = std::max(1, perSm * sms);
+        }
+        grid = std::min(grid, g);
+        cudaError_t e = cudaMemsetAsync(h->dWork, 0, sizeof(unsigned int), st);
+        if (e != cudaSuccess) return e;
+    }
+    sv.fn<<<grid, block, 0, st>>>(D, ticks);
+    return cudaGetLastError();
+}
+
 rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
     if (!h || ticks < 0) return fail(h, RSB_ERR_INVALID, "bad tick count");
     if (ticks == 0) return RSB_OK;
@@ -584,9 +636,7 @@ rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
         RSB_CUDA(cudaGetLastError());
         D.cull = h->dCull;
     }
-    int block = kStepBlocks[h->stepBlock], grid = (h->N + block - 1) / block;
-    kStepVariants[h->stepVariant].fn<<<grid, block, 0, st>>>(D, ticks);
-    RSB_CUDA(cudaGetLastError());
+    RSB_CUDA(launchStep(h, D, h->stepVariant, h->stepBlock, ticks, st));
     h->stats.ticks_simulated += (uint64_t)h->N * ticks;
     return RSB_OK;
 }
@@ -620,12 +670,8 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
                 if (e == cudaSuccess) e = cudaMemcpyAsync(D.pad, h->dPad, wPad * 4, cudaMemcpyDeviceToDevice, h->stream);
                 if (e == cudaSuccess)
                     e = cudaMemcpyAsync(D.arena, h->dArena, wArena * 4, cudaMemcpyDeviceToDevice, h->stream);
-                const int block = kStepBlocks[b], grid = (h->N + block - 1) / block;
                 if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
-                if (e == cudaSuccess) {
-                    kStepVariants[v].fn<<<grid, block, 0, h->stream>>>(D, ticks);
-                    e = cudaGetLastError();
-                }
+                if (e == cudaSuccess) e = launchStep(h, D, v, b, ticks, h->stream);
                 if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
                 if (e == cudaSuccess) e = cudaEventSynchronize(e1);
                 float t = 0.f;
@@ -637,7 +683,8 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
                 ms = std::min(ms, t);
             }
             if (st != RSB_OK) break;
-            if (out && n < cap) out[n] = rsb_tune_entry{kStepVariants[v].minBlocks, kStepBlocks[b], ms};
+            if (out && n < cap)
+                out[n] = rsb_tune_entry{kStepVariants[v].minBlocks, kStepBlocks[b], ms, kStepVariants[v].persistent ? 1 : 0};
             n++;
             if (ms < best) { best = ms; bestV = v; bestB = b; }
         }
@@ -648,6 +695,19 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
     h->stepBlock = bestB;
     if (count) *count = n;
     return RSB_OK;
+}
+
+rsb_status rsb_set_step_config(rsb_handle* h, const rsb_tune_entry* cfg) {
+    if (!h || !cfg) return RSB_ERR_INVALID;
+    for (int v = 0; v < kNumStepVariants; v++)
+        for (int b = 0; b < kNumStepBlocks; b++)
+            if (kStepVariants[v].minBlocks == cfg->min_blocks && kStepBlocks[b] == cfg->block &&
+                kStepVariants[v].persistent == (cfg->persistent != 0)) {
+                h->stepVariant = v;
+                h->stepBlock = b;
+                return RSB_OK;
+            }
+    return fail(h, RSB_ERR_INVALID, "rsb_set_step_config: no such launch configuration");
 }
 
 rsb_status rsb_sync(rsb_handle* h) {

@@ -149,7 +149,7 @@ def culler_config(**kw) -> CullerConfig:
 
 
 class TuneEntry(C.Structure):
-    _fields_ = [("min_blocks", C.c_int32), ("block", C.c_int32), ("ms", C.c_float)]
+    _fields_ = [("min_blocks", C.c_int32), ("block", C.c_int32), ("ms", C.c_float), ("persistent", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -199,6 +199,7 @@ _SIGS = {
     "rsb_step": [_P, C.c_int32, _P],
     "rsb_reset_done": [_P, C.c_uint64, C.c_int32, _P],
     "rsb_autotune": [_P, C.c_int32, _P, C.c_int32, _P],
+    "rsb_set_step_config": [_P, _P],
     "rsb_culler_log": [_P, _P],
     "rsb_set_cull_mode": [_P, C.c_int32],
     "rsb_culler_train": [_P, _P, _P],
@@ -536,7 +537,13 @@ class Batch:
         out = (TuneEntry * 32)()
         n = C.c_int32()
         self._check(self.lib.rsb_autotune(self._h, ticks, out, 32, C.byref(n)))
-        return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms} for e in out[:n.value]]
+        return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms, "persistent": e.persistent}
+                for e in out[:n.value]]
+
+    def set_step_config(self, min_blocks: int, block: int, persistent: bool = False):
+        """rsb_set_step_config: pins a launch configuration of the step kernel."""
+        e = TuneEntry(min_blocks=min_blocks, block=block, ms=0.0, persistent=1 if persistent else 0)
+        self._check(self.lib.rsb_set_step_config(self._h, C.byref(e)))
 
     # ---------------------------------------------------------------- learned culler
     def set_cull_mode(self, mode: int):

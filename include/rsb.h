@@ -323,6 +323,7 @@ typedef struct rsb_tune_entry {
     int32_t min_blocks;   /* register budget: at least this many 128-thread blocks per SM */
     int32_t block;        /* threads per block (one arena per thread) */
     float ms;             /* best of two timed launches of `ticks` ticks */
+    int32_t persistent;   /* 1: resident-size grid whose warps claim 32 arenas at a time */
 } rsb_tune_entry;
 
 /* Times every launch configuration of the step kernel on a device copy of the current
@@ -330,6 +331,9 @@ typedef struct rsb_tune_entry {
  * rsb_step calls, and reports every candidate in out[0..cap).  Allocates the scratch copy
  * of the state on its first call.  No counterpart in the reference. */
 rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32_t cap, int32_t* count);
+/* Selects a launch configuration (min_blocks, block, persistent as rsb_autotune reports them),
+ * e.g. one tuned in an earlier run; RSB_ERR_INVALID if no such configuration exists. */
+rsb_status rsb_set_step_config(rsb_handle* h, const rsb_tune_entry* cfg);
 
 /* ---- learned culler (no counterpart in the reference) ----
  * A 3 -> 64 -> 64 -> 1 MLP (BF16 weights, FP32 accumulation) estimates the distance (uu)

@@ -761,6 +761,7 @@ rsb_status rsb_compute_gae_host(const float*, const int8_t*, const float*, int32
 }
 
 // The CPU oracle has a single configuration.
+rsb_status rsb_set_step_config(rsb_handle* h, const rsb_tune_entry* cfg) { return h && cfg ? RSB_OK : RSB_ERR_INVALID; }
 rsb_status rsb_autotune(rsb_handle* h, int32_t, rsb_tune_entry*, int32_t, int32_t* count) {
     if (!h) return RSB_ERR_INVALID;
     if (count) *count = 0;

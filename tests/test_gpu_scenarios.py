@@ -1,0 +1,250 @@
+"""The reference's CPU-vs-GPU scenario suite (RocketSimCuda/tests/compare_cpu_cuda.cpp:425-796),
+restated as engine against oracle: the same scenarios, durations, per-tick controls and
+tolerance sets, and the same end-of-run metrics (Euclidean position / velocity difference of
+the ball and of the worst car, forward-vector angle, boost, on-ground and demo flags, goal
+flag and team; compare_cpu_cuda.cpp:151-178, 222-235).
+
+Each scenario starts, as the reference's harness does, from a kickoff reset of one arena that
+both sides share.  The engine lays out symmetric teams, so a scenario written for one blue car
+runs in a 1v1 arena whose orange car is parked at rest, away from every boost pad, where it
+touches nothing during the run.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from gpu_util import reference_reverse_order, vec
+
+pytestmark = pytest.mark.gpu
+
+DEFAULT_TOL = (0.5, 0.5, 0.5, 0.5, 0.2, 0.05)  # ball pos, ball vel, car pos, car vel, forward deg, boost
+PARK = (-2700.0, 3300.0)
+PI = np.float32(np.pi)
+
+
+def _yaw_rot(rec, yaw):
+    cy, sy = np.cos(np.float32(yaw)), np.sin(np.float32(yaw))
+    for f, v in (("forward", (cy, sy, 0.0)), ("right", (-sy, cy, 0.0)), ("up", (0.0, 0.0, 1.0))):
+        for k, comp in enumerate("xyz"):
+            rec["rot"][f][comp] = v[k]
+
+
+def _set3(rec, field, v):
+    for k, comp in enumerate("xyz"):
+        rec[field][comp] = v[k]
+
+
+def _ball(rsb, x, y, z, vx, vy, vz):
+    b = np.zeros(1, rsb.BALL_DTYPE)[0]
+    for f, v in (("forward", (1, 0, 0)), ("right", (0, 1, 0)), ("up", (0, 0, 1))):
+        _set3(b["rot"], f, v)
+    _set3(b, "pos", (x, y, z))
+    _set3(b, "vel", (vx, vy, vz))
+    return b
+
+
+def ctl(**kw):
+    return kw
+
+
+# ---------------------------------------------------------------- scenario table
+
+def flip_controls(pitch=0.0, yaw=0.0, roll=0.0, throttle_flip=False, throttle_after=False):
+    def f(t):
+        if t < 3:
+            return ctl(jump=1)
+        if 8 <= t < 11:
+            return ctl(jump=1, pitch=pitch, yaw=yaw, roll=roll, throttle=1.0 if throttle_flip else 0.0)
+        return ctl(throttle=1.0 if throttle_after else 0.0)
+    return f
+
+
+def _setup_ball(x, y, z, vx, vy, vz):
+    def s(rsb, car, ball):
+        ball[0] = _ball(rsb, x, y, z, vx, vy, vz)
+    return s
+
+
+def _aerial(rsb, car, ball):
+    c = car[0]
+    _set3(c, "pos", (500.0, -1000.0, 700.0))
+    _yaw_rot(c, PI * np.float32(0.25))
+    _set3(c, "vel", (0.0, 0.0, 150.0))
+    _set3(c, "ang_vel", (0.0, 0.0, 0.0))
+    c["is_on_ground"] = 0
+    c["boost"] = 100.0
+
+
+def _wall(rsb, car, ball):
+    c = car[0]
+    _set3(c, "pos", (np.float32(4096.0) - np.float32(17.01), -800.0, 600.0))
+    _set3(c["rot"], "forward", (0.0, 0.0, 1.0))
+    _set3(c["rot"], "right", (0.0, 1.0, 0.0))
+    _set3(c["rot"], "up", (-1.0, 0.0, 0.0))
+    _set3(c, "vel", (0.0, 0.0, 500.0))
+    _set3(c, "ang_vel", (0.0, 0.0, 0.0))
+    c["boost"] = 50.0
+
+
+def _dribble(rsb, car, ball):
+    c = car[0]
+    _set3(c, "pos", (0.0, 0.0, 17.01))
+    _yaw_rot(c, 0.0)
+    _set3(c, "vel", (300.0, 0.0, 0.0))
+    c["boost"] = 30.0
+    f = np.float32
+    z = f(17.01) + f(38.66) * f(0.5) + f(20.755) - f(17.01) + f(92.0) + f(40.0)
+    ball[0] = _ball(rsb, 20.0, 0.0, z, 300.0, 0.0, 0.0)
+
+
+def _demo(rsb, car, ball):
+    c0, c1 = car[0], car[1]
+    _set3(c0, "pos", (-1500.0, 0.0, float(c0["pos"]["z"])))
+    _yaw_rot(c0, 0.0)
+    _set3(c0, "vel", (2250.0, 0.0, 0.0))
+    c0["is_supersonic"] = 1
+    c0["boost"] = 100.0
+    _set3(c1, "pos", (-200.0, 10.0, float(c1["pos"]["z"])))
+    _yaw_rot(c1, PI * np.float32(0.5))
+    _set3(c1, "vel", (0.0, 0.0, 0.0))
+
+
+def _car_ball(rsb, car, ball):
+    c = car[0]
+    _set3(c, "pos", (0.0, -1400.0, float(c["pos"]["z"])))
+    _yaw_rot(c, PI * np.float32(0.5))
+    _set3(c, "vel", (0.0, 0.0, 0.0))
+    _set3(c, "ang_vel", (0.0, 0.0, 0.0))
+    c["boost"] = 100.0
+    ball[0] = _ball(rsb, 0.0, -220.0, 93.15, 0.0, 0.0, 0.0)
+
+
+def _pad(rsb, car, ball):
+    c = car[0]
+    _set3(c, "pos", (0.0, -2920.0, float(c["pos"]["z"])))
+    _yaw_rot(c, PI * np.float32(0.5))
+    _set3(c, "vel", (0.0, 650.0, 0.0))
+    _set3(c, "ang_vel", (0.0, 0.0, 0.0))
+    c["boost"] = 0.0
+
+
+def _bump(rsb, car, ball):
+    c0, c1 = car[0], car[1]
+    _set3(c0, "pos", (-600.0, 0.0, float(c0["pos"]["z"])))
+    _yaw_rot(c0, 0.0)
+    _set3(c0, "vel", (1200.0, 0.0, 0.0))
+    c0["boost"] = 100.0
+    _set3(c1, "pos", (600.0, 0.0, float(c1["pos"]["z"])))
+    _yaw_rot(c1, PI)
+    _set3(c1, "vel", (-1200.0, 0.0, 0.0))
+    c1["boost"] = 100.0
+
+
+DROP = _setup_ball(0.0, 0.0, 500.0, 0.0, 0.0, -1.0)
+FLIP_TOL = (0.5, 0.5, 8.0, 35.0, 3.0, 0.05)
+
+# name: (two cars, ticks, tolerances (DEFAULT_TOL order), setup, controls of car 0 per tick or None)
+SCENARIOS = {
+    "ball_drop_1": (False, 1, DEFAULT_TOL, DROP, None),
+    "ball_drop_120": (False, 120, DEFAULT_TOL, DROP, None),
+    "ball_drop_1440": (False, 1440, DEFAULT_TOL, DROP, None),
+    "kickoff_idle_120": (False, 120, DEFAULT_TOL, None, None),
+    "kickoff_idle_600": (False, 600, DEFAULT_TOL, None, None),
+    "boost_drive_60": (False, 60, DEFAULT_TOL, None, lambda t: ctl(throttle=1.0, boost=1)),
+    "boost_drive_120": (False, 120, DEFAULT_TOL, None, lambda t: ctl(throttle=1.0, boost=1)),
+    "jump_hold_30": (False, 30, DEFAULT_TOL, None, lambda t: ctl(jump=int(t < 6))),
+    "double_jump_45": (False, 45, DEFAULT_TOL, None, lambda t: ctl(jump=int(t < 3 or 12 <= t < 15))),
+    "front_flip_60": (False, 60, (0.5, 0.5, 8.0, 30.0, 3.0, 0.05), None,
+                      flip_controls(pitch=-1.0, throttle_flip=True, throttle_after=True)),
+    "diag_flip_60": (False, 60, FLIP_TOL, None, flip_controls(pitch=-0.7, yaw=0.7)),
+    "side_flip_60": (False, 60, FLIP_TOL, None, flip_controls(yaw=1.0)),
+    "back_flip_50": (False, 50, DEFAULT_TOL, None, flip_controls(pitch=1.0)),
+    "stall_flip_55": (False, 55, DEFAULT_TOL, None, flip_controls(yaw=1.0, roll=-1.0)),
+    "steer_drive_150": (False, 150, DEFAULT_TOL, None, lambda t: ctl(throttle=1.0, steer=0.6)),
+    "powerslide_turn_120": (False, 120, DEFAULT_TOL, None,
+                            lambda t: ctl(throttle=1.0, steer=1.0 if t >= 40 else 0.0, handbrake=int(t >= 40))),
+    "aerial_control_150": (False, 150, DEFAULT_TOL, _aerial,
+                           lambda t: ctl(boost=int(t % 10 < 6), pitch=0.45 if t < 60 else -0.2, yaw=0.3,
+                                         roll=-0.8 if 80 <= t < 110 else 0.0)),
+    "wall_drive_100": (False, 100, DEFAULT_TOL, _wall, lambda t: ctl(throttle=1.0)),
+    "ball_corner_bounce_150": (False, 150, DEFAULT_TOL, _setup_ball(2800.0, -4000.0, 300.0, 1300.0, -1200.0, 0.0), None),
+    "ball_roll_300": (False, 300, DEFAULT_TOL, _setup_ball(-1000.0, 1000.0, 93.15, 900.0, -300.0, 0.0), None),
+    "ball_ceiling_bounce_120": (False, 120, DEFAULT_TOL, _setup_ball(0.0, 800.0, 1600.0, 200.0, 0.0, 1400.0), None),
+    "dribble_roof_90": (False, 90, DEFAULT_TOL, _dribble, lambda t: ctl(throttle=0.6)),
+    # the victim's respawn place is random in the reference: flags and timers only
+    "supersonic_demo_40": (True, 40, (0.5, 0.5, 1e9, 1e9, 180.0, 100.0), _demo, lambda t: ctl(throttle=1.0, boost=1)),
+    "car_ball_hit_60": (False, 60, DEFAULT_TOL, _car_ball, lambda t: ctl(throttle=1.0, boost=1)),
+    "ball_wall_bounce_120": (False, 120, DEFAULT_TOL, _setup_ball(3500.0, 0.0, 400.0, 1800.0, 0.0, 0.0), None),
+    "boost_pad_pickup_45": (False, 45, DEFAULT_TOL, _pad, lambda t: ctl(throttle=1.0)),
+    "goal_detection_20": (False, 20, (3.0, 15.0, 0.5, 0.5, 0.2, 0.05), _setup_ball(0.0, 5000.0, 100.0, 0.0, 2000.0, 0.0),
+                          None),
+    "car_car_bump_30": (True, 30, DEFAULT_TOL, _bump, lambda t: ctl()),
+}
+
+
+def _pair(pkg, oracle_lib, meshes_dir, seed):
+    """One 1v1 arena on each side, from the oracle's kickoff; retried until the reference visits
+    the two cars in reverse creation order (the engine's order)."""
+    rsb = pkg.rsb
+    for k in range(8):
+        eng = rsb.Batch(pkg.engine_library(), 1, team_size=1, meshes_path=meshes_dir)
+        ora = rsb.Batch(oracle_lib, 1, team_size=1, meshes_path=meshes_dir, threads=1)
+        if reference_reverse_order(ora, pkg)[0]:
+            break
+    ora.reset_all(seed, rsb.RSB_RESET_KICKOFF)
+    cars, balls, pads = ora.get_cars(), ora.get_balls(), ora.get_pads()
+    for b in (eng, ora):
+        b.set_cars(cars)
+        b.set_balls(balls)
+        b.set_pads(pads)
+    return eng, ora
+
+
+@pytest.mark.parametrize("name", list(SCENARIOS))
+def test_reference_scenario(pkg, oracle_lib, meshes_dir, name):
+    rsb = pkg.rsb
+    two_cars, ticks, tol, setup, controls = SCENARIOS[name]
+    eng, ora = _pair(pkg, oracle_lib, meshes_dir, seed=7)
+    cars, balls = ora.get_cars(), ora.get_balls()
+    if not two_cars:  # park the orange car
+        _set3(cars[1], "pos", (PARK[0], PARK[1], 17.01))
+        _yaw_rot(cars[1], 0.0)
+        _set3(cars[1], "vel", (0.0, 0.0, 0.0))
+        _set3(cars[1], "ang_vel", (0.0, 0.0, 0.0))
+    if setup:
+        setup(rsb, cars, balls)
+    for b in (eng, ora):
+        b.set_cars(cars)
+        b.set_balls(balls)
+    c = np.zeros(2, rsb.CONTROLS_DTYPE)
+    if controls is None:
+        for b in (eng, ora):
+            b.set_controls(c)
+            b.step(ticks)
+    else:
+        for t in range(ticks):
+            c[:] = 0
+            for k, v in controls(t).items():
+                c[0][k] = v
+            for b in (eng, ora):
+                b.set_controls(c)
+                b.step(1)
+    ce, co = eng.get_cars(), ora.get_cars()
+    be, bo = eng.get_balls(), ora.get_balls()
+    ie, io = eng.get_arena_info()[0], ora.get_arena_info()[0]
+    ball_pos = float(np.linalg.norm(vec(be, "pos") - vec(bo, "pos")))
+    ball_vel = float(np.linalg.norm(vec(be, "vel") - vec(bo, "vel")))
+    car_pos = float(np.linalg.norm(vec(ce, "pos") - vec(co, "pos"), axis=1).max())
+    car_vel = float(np.linalg.norm(vec(ce, "vel") - vec(co, "vel"), axis=1).max())
+    fe, fo = vec(ce["rot"], "forward"), vec(co["rot"], "forward")
+    cosang = np.clip((fe * fo).sum(1) / np.maximum(np.linalg.norm(fe, axis=1) * np.linalg.norm(fo, axis=1), 1e-6), -1, 1)
+    fwd = float(np.degrees(np.arccos(cosang)).max())
+    boost = float(np.abs(ce["boost"] - co["boost"]).max())
+    got = dict(ball_pos=ball_pos, ball_vel=ball_vel, car_pos=car_pos, car_vel=car_vel, fwd=fwd, boost=boost)
+    print(f"SCENARIO {name} " + " ".join(f"{k}={v:.3g}" for k, v in got.items()))
+    for (k, v), limit in zip(got.items(), tol):
+        assert v <= limit, f"{name}: {k} differs by {v:.4g} (tolerance {limit}); {got}"
+    assert np.array_equal(ce["is_on_ground"], co["is_on_ground"]), f"{name}: on-ground flags differ"
+    assert np.array_equal(ce["is_demoed"], co["is_demoed"]), f"{name}: demo flags differ"
+    assert ie["goal_scored"] == io["goal_scored"] and ie["goal_team"] == io["goal_team"], f"{name}: goal differs"

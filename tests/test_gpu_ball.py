@@ -74,3 +74,18 @@ def test_goal_flag_matches_oracle(pkg, oracle_lib, meshes_dir):
         ia, ib = eng.get_arena_info(), ora.get_arena_info()
         np.testing.assert_array_equal(ia["goal_scored"], ib["goal_scored"])
         np.testing.assert_array_equal(ia["goal_team"], ib["goal_team"])
+
+
+def test_floor_bounce_invariants_and_oracle(pkg, oracle_lib, meshes_dir):
+    """The reference's floor-bounce invariants (bounce, no tunnelling, no energy gain) on the
+    engine, and the same end state as the oracle."""
+    from test_oracle_pins import bounce_invariants
+
+    rsb = pkg.rsb
+    eng = rsb.Batch(pkg.engine_library(), 1, team_size=0, meshes_path=meshes_dir)
+    ora = rsb.Batch(oracle_lib, 1, team_size=0, meshes_path=meshes_dir, threads=1)
+    be = bounce_invariants(eng)
+    bo = bounce_invariants(ora)
+    assert be[0] and be[1] >= 0.5 * 91.25 and be[2] <= be[3] * 1.001, be
+    assert abs(be[1] - bo[1]) < 1e-3 and abs(be[2] - bo[2]) <= 1e-4 * bo[2]
+    assert np.allclose(vec(eng.get_balls(), "pos"), vec(ora.get_balls(), "pos"), atol=1e-2)

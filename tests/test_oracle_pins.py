@@ -278,3 +278,31 @@ def test_soccar_mesh_hashes(meshes_dir):
 
 def test_oracle_library_is_the_reference_build():
     assert os.path.exists(ORACLE_LIB)
+
+
+def bounce_invariants(b, ticks=120):
+    """Ball thrown down from 1,000 uu at 1,758 uu/s onto the floor (ball_floor_bounce_120t
+    in RocketSimCuda/tests/reports/cpu_parity_report.txt): it bounces, does not tunnel through the
+    floor (its centre stays above half its radius; Bullet's discrete contact lets it sink about
+    11 uu at this speed before pushing it out), and its mechanical energy per unit mass never
+    grows by more than 0.1 %."""
+    balls = b.get_balls()
+    _set_identity(balls)
+    for k, c in enumerate("xyz"):
+        balls["pos"][c], balls["vel"][c], balls["ang_vel"][c] = (0.0, 0.0, 1000.0)[k], (0.0, 0.0, -1757.84)[k], 0.0
+    b.set_balls(balls)
+    e0 = 0.5 * 1757.84 ** 2 + 650.0 * 1000.0  # 2.195e6, the report's E0
+    min_z, max_e, bounced = 1e9, 0.0, False
+    for _ in range(ticks):
+        b.step(1)
+        s = b.get_balls()[0]
+        z, v = float(s["pos"]["z"]), _v(s, "vel")
+        min_z = min(min_z, z)
+        max_e = max(max_e, 0.5 * float(v @ v) + 650.0 * z)
+        bounced |= v[2] > 0
+    return bounced, min_z, max_e, e0
+
+
+def test_ball_floor_bounce_invariants(rsb, oracle_lib, meshes_dir):
+    bounced, min_z, max_e, e0 = bounce_invariants(_batch(rsb, oracle_lib, meshes_dir, team_size=0))
+    assert bounced and min_z >= 0.5 * 91.25 and max_e <= e0 * 1.001, (bounced, min_z, max_e, e0)

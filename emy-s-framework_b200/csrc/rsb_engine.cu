@@ -941,6 +941,15 @@ rsb_status rsb_get_car_at(rsb_handle* h, int32_t arena, int32_t car, rsb_car_sta
     return RSB_OK;
 }
 
+rsb_status rsb_set_car_controls_at(rsb_handle* h, int32_t arena, int32_t car, const rsb_controls* in) {
+    if (!h || !in || !carIndex(h, arena, car)) return fail(h, RSB_ERR_INVALID, "rsb_set_car_controls_at: no such car");
+    RSB_CUDA(cudaSetDevice(h->device));
+    RSB_CUDA(cudaMemcpyAsync(h->dControls + h->carOffset[arena] + car, in, sizeof(rsb_controls),
+                             cudaMemcpyHostToDevice, h->stream));
+    RSB_CUDA(cudaStreamSynchronize(h->stream));  // the caller's struct may go away on return
+    return RSB_OK;
+}
+
 rsb_status rsb_set_car_at(rsb_handle* h, int32_t arena, int32_t car, const rsb_car_state* in) {
     if (!h || !in || !carIndex(h, arena, car)) return fail(h, RSB_ERR_INVALID, "rsb_set_car_at: no such car");
     RSB_CUDA(cudaSetDevice(h->device));

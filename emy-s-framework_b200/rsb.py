@@ -225,6 +225,7 @@ _SIGS = {
     "rsb_get_arena_info": [_P, _P, C.c_int32],
     "rsb_copy_outputs": [_P, _P, _P, _P, _P],
     "rsb_get_car_at": [_P, C.c_int32, C.c_int32, _P],
+    "rsb_set_car_controls_at": [_P, C.c_int32, C.c_int32, _P],
     "rsb_set_car_at": [_P, C.c_int32, C.c_int32, _P],
     "rsb_get_ball_at": [_P, C.c_int32, _P],
     "rsb_set_ball_at": [_P, C.c_int32, _P],

@@ -311,6 +311,9 @@ rsb_status rsb_get_arena_info(rsb_handle* h, rsb_arena_info* out, int32_t n);
  * stream); the setters launch one small kernel on the handle's stream with the same
  * conversion as the whole-batch setters, so other arenas are not touched. */
 rsb_status rsb_get_car_at(rsb_handle* h, int32_t arena, int32_t car, rsb_car_state* out);
+/* RocketSimCudaBatch::SetCarControls (RocketSimCuda.h:286): one car's controls, the others
+ * unchanged; takes effect at the next rsb_step (ordered on the handle's stream). */
+rsb_status rsb_set_car_controls_at(rsb_handle* h, int32_t arena, int32_t car, const rsb_controls* in);
 rsb_status rsb_set_car_at(rsb_handle* h, int32_t arena, int32_t car, const rsb_car_state* in);
 rsb_status rsb_get_ball_at(rsb_handle* h, int32_t arena, rsb_ball_state* out);
 rsb_status rsb_set_ball_at(rsb_handle* h, int32_t arena, const rsb_ball_state* in);

@@ -497,6 +497,11 @@ rsb_status rsb_get_car_at(rsb_handle* h, int32_t a, int32_t c, rsb_car_state* ou
     *out = fromCarState(car->GetState(), car->team, car->id);
     return RSB_OK;
 }
+rsb_status rsb_set_car_controls_at(rsb_handle* h, int32_t a, int32_t c, const rsb_controls* in) {
+    if (!validArena(h, a) || !in || c < 0 || c >= (int32_t)h->cars[a].size()) return fail(h, RSB_ERR_INVALID, "no such car");
+    h->controls[(size_t)h->carOffset[a] + c] = *in;
+    return RSB_OK;
+}
 rsb_status rsb_set_car_at(rsb_handle* h, int32_t a, int32_t c, const rsb_car_state* in) {
     if (!validArena(h, a) || !in || c < 0 || c >= (int32_t)h->cars[a].size()) return fail(h, RSB_ERR_INVALID, "no such car");
     h->cars[a][c]->SetState(toCarState(*in));

@@ -407,6 +407,22 @@ def run_ours(args, rank, world, dist):
                 "reference_style_host_capture_ms": statistics.median(host_ms)}
         batch.ring_configure(depth=0)
 
+    # ball prediction (BallPredTracker's ball-only rollout, the one VantaObs reads at 1/2/3 s)
+    # of every arena's ball, slices left on the device
+    pred = None
+    if wl.preset == "c3" and not args.no_pred:
+        pred_ms = []
+        for k in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            batch.predict_ball((120, 240, 360), to_host=False, stream=sp)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            pred_ms.append(e0.elapsed_time(e1))
+        pms = statistics.median(pred_ms[1:])
+        pred = {"arenas": wl.num_arenas, "ticks": 360, "slices": [120, 240, 360], "ms": pms,
+                "ball_ticks_per_s": wl.num_arenas * 360 / pms * 1e3}
+
     # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
     # state read + written per launch (the library reports it), over the kernel's own time
     alg_bytes = batch.stats()["state_bytes_per_step"]
@@ -437,6 +453,7 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": steps * (6 if learned is not None else 5),
         "learned_cull": learned,
         "state_ring": ring,
+        "ball_prediction": pred,
         "autotune": tune,
         "clocks": clocks[-1],
         "clocks_exact": clocks[0],
@@ -720,6 +737,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gae", action="store_true", help="skip the GAE measurement of the c3 line")
     ap.add_argument("--no-ring", action="store_true", help="skip the state-ring measurement of the c3 line")
+    ap.add_argument("--no-pred", action="store_true", help="skip the ball-prediction measurement of the c3 line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

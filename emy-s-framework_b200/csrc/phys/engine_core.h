@@ -40,9 +40,7 @@ RSB_HD void initBodyCommon(Body& b) {
     b.spNormal = v3zero();
 }
 
-RSB_HD void loadBall(const EngineView& D, int a, Body& b) {
-    BallP p;
-    loadPlanes(p, D.ball, a, D.N);
+RSB_HD void ballBodyOf(const EngineView& D, const BallP& p, Body& b) {
     b.xf = xfFromP(p.pos, p.rot);
     b.lin = V3{p.lin[0], p.lin[1], p.lin[2]};
     b.ang = V3{p.ang[0], p.ang[1], p.ang[2]};
@@ -63,7 +61,13 @@ RSB_HD void loadBall(const EngineView& D, int a, Body& b) {
     b.bpMin = b.bpMax = b.xf.o;
 }
 
-RSB_HD void storeBall(const EngineView& D, int a, const Body& b) {
+RSB_HD void loadBall(const EngineView& D, int a, Body& b) {
+    BallP p;
+    loadPlanes(p, D.ball, a, D.N);
+    ballBodyOf(D, p, b);
+}
+
+RSB_HD BallP ballRecordOf(const Body& b) {
     BallP p;
     xfToP(b.xf, p.pos, p.rot);
     p.lin[0] = b.lin.x; p.lin[1] = b.lin.y; p.lin[2] = b.lin.z;
@@ -73,6 +77,11 @@ RSB_HD void storeBall(const EngineView& D, int a, const Body& b) {
     p.cj = b.cj;
     p.ck = b.ck;
     p.regStamp = b.regStamp;
+    return p;
+}
+
+RSB_HD void storeBall(const EngineView& D, int a, const Body& b) {
+    BallP p = ballRecordOf(b);
     storePlanes(p, D.ball, a, D.N);
 }
 

@@ -128,6 +128,8 @@ struct rsb_handle {
     unsigned int* dWork = nullptr;  // claim counter of the persistent step kernel
     int persistGrid[8][4] = {};     // resident blocks (all SMs) per persistent variant and block size
     uint32_t* dStage = nullptr;     // staging of the per-arena getters
+    rsb_ball_state* dPred = nullptr;  // ball prediction slices [num_arenas][n_slices]
+    size_t predCap = 0;
     size_t stageWords = 0;
     EnvTables tables{};
     bool hasRewards = false;
@@ -323,6 +325,50 @@ __global__ void setPadsKernel(uint32_t* pad, int a, int N, PadSet s) {
     pp.cooldown = s.p[p].cooldown;
     pp.bits = (s.p[p].is_active ? 1u : 0u) | (s.p[p].prev_locked_car_id << 8);
     storePlanes(pp, pad, p * N + a, N * NUM_PADS);
+}
+
+struct PredSlices {
+    int32_t t[RSB_MAX_PRED_SLICES];
+    int32_t n;
+};
+
+// BallPredTracker::ForceUpdateAllPred (BallPredTracker.cpp:80-88) for every arena at once: the
+// arena's ball passes through Ball::GetState / Ball::SetState into a world of its own with no
+// cars, which steps one tick at a time (Arena::Step of a ball-only arena); out[a * n + k] is the
+// ball after s.t[k] ticks.  The arena's own records are only read.
+__global__ void __launch_bounds__(128) predictBallKernel(EngineView D, PredSlices s, rsb_ball_state* out) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= D.N) return;
+    ArenaSim A;
+    EpaWork epa;
+    World& W = A.W;
+    W.epa = &epa;
+    W.S = &D.S;
+    W.P = &D.P;
+    A.teamSize = A.numCars = 0;
+    W.nc = 0;
+    W.nb = 1;
+    W.status = 0;
+    W.noRot[0] = 1;
+    BallP p;
+    loadPlanes(p, D.ball, a, D.N);
+    applyBallState(p, ballStateOf(p));
+    ballBodyOf(D, p, W.b[0]);
+    A.tickCount = 0;
+    A.status = 0;
+    A.goalTeam = -1;
+    A.touchedMask = 0;
+    A.rngKey = 0;
+    W.cull = 0;
+    W.cullAudit = 0;
+    W.nStatic = W.nCulled = W.nMissed = 0;
+    W.cullMissed = 0;
+    W.nRows = 0;
+    int t = 0;
+    for (int k = 0; k < s.n; k++) {
+        for (; t < s.t[k]; t++) arenaTick(A);
+        out[(size_t)a * s.n + k] = ballStateOf(ballRecordOf(W.b[0]));
+    }
 }
 
 __global__ void expandActionsKernel(const int32_t* idx, const rsb_controls* lut, int lutCount, rsb_controls* out, int n) {
@@ -578,7 +624,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
     cudaFree(h->dTris);
     cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
-    cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage); cudaFree(h->dWork);
+    cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage); cudaFree(h->dWork); cudaFree(h->dPred);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return RSB_OK;
@@ -638,6 +684,39 @@ rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
     }
     RSB_CUDA(launchStep(h, D, h->stepVariant, h->stepBlock, ticks, st));
     h->stats.ticks_simulated += (uint64_t)h->N * ticks;
+    return RSB_OK;
+}
+
+rsb_status rsb_predict_ball(rsb_handle* h, const int32_t* slice_ticks, int32_t n_slices, rsb_ball_state* out,
+                            size_t out_count, void* stream) {
+    if (!h || !slice_ticks || n_slices < 1 || n_slices > RSB_MAX_PRED_SLICES)
+        return fail(h, RSB_ERR_INVALID, "rsb_predict_ball: 1..8 slice ticks are required");
+    PredSlices s{};
+    s.n = n_slices;
+    for (int k = 0; k < n_slices; k++) {
+        const int32_t prev = k ? slice_ticks[k - 1] : 0;
+        if (slice_ticks[k] <= prev || slice_ticks[k] > RSB_MAX_PRED_TICKS)
+            return fail(h, RSB_ERR_INVALID, "rsb_predict_ball: slice ticks must rise, from 1 to 4096");
+        s.t[k] = slice_ticks[k];
+    }
+    const size_t need = (size_t)h->N * n_slices;
+    if (out && out_count != need) return fail(h, RSB_ERR_INVALID, "rsb_predict_ball: out_count must be num_arenas * n_slices");
+    RSB_CUDA(cudaSetDevice(h->device));
+    if (h->predCap < need) {
+        cudaFree(h->dPred);
+        h->dPred = nullptr;
+        h->predCap = 0;
+        if (cudaMalloc((void**)&h->dPred, need * sizeof(rsb_ball_state)) != cudaSuccess)
+            return fail(h, RSB_ERR_NOMEM, "rsb_predict_ball: allocation failed");
+        h->predCap = need;
+    }
+    cudaStream_t st = pick(h, stream);
+    predictBallKernel<<<(h->N + 127) / 128, 128, 0, st>>>(devView(h), s, h->dPred);
+    RSB_CUDA(cudaGetLastError());
+    if (out) {
+        RSB_CUDA(cudaMemcpyAsync(out, h->dPred, need * sizeof(rsb_ball_state), cudaMemcpyDeviceToHost, st));
+        RSB_CUDA(cudaStreamSynchronize(st));
+    }
     return RSB_OK;
 }
 
@@ -1541,6 +1620,7 @@ rsb_status rsb_device_ptr(rsb_handle* h, int32_t which, void** out) {
         case RSB_BUF_TERMINALS: *out = h->dTerminals; return RSB_OK;
         case RSB_BUF_CONTROLS: *out = h->dControls; return RSB_OK;
         case RSB_BUF_ACTIONS: *out = h->dActions; return RSB_OK;
+        case RSB_BUF_BALL_PRED: *out = h->dPred; return RSB_OK;
         default: return fail(h, RSB_ERR_INVALID, "unknown buffer");
     }
 }

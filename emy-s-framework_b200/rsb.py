@@ -27,7 +27,9 @@ RSB_STATIC_ACTIONS_MAX = 65536 * 6
 RSB_OBS_BASE = 51
 RSB_OBS_PER_CAR = 29
 
-RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS = range(6)
+RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS, RSB_BUF_BALL_PRED = range(7)
+RSB_MAX_PRED_SLICES = 8
+RSB_MAX_PRED_TICKS = 4096
 RSB_CULL_EXACT, RSB_CULL_LEARNED, RSB_CULL_LEARNED_AUDIT = 0, 1, 2
 RSB_CULLER_PARAMS = 4481
 RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT = 0, 1, 2
@@ -228,6 +230,7 @@ _SIGS = {
     "rsb_set_car_controls_at": [_P, C.c_int32, C.c_int32, _P],
     "rsb_set_car_at": [_P, C.c_int32, C.c_int32, _P],
     "rsb_get_ball_at": [_P, C.c_int32, _P],
+    "rsb_predict_ball": [_P, _P, C.c_int32, _P, C.c_size_t, _P],
     "rsb_set_ball_at": [_P, C.c_int32, _P],
     "rsb_get_pads_at": [_P, C.c_int32, _P],
     "rsb_set_pads_at": [_P, C.c_int32, _P],
@@ -696,6 +699,19 @@ class Batch:
     def get_balls(self) -> np.ndarray:
         out = np.zeros(self.num_arenas, BALL_DTYPE)
         self._check(self.lib.rsb_get_balls(self._h, _ptr(out), self.num_arenas))
+        return out
+
+    def predict_ball(self, slice_ticks=(120, 240, 360), to_host: bool = True, stream=None):
+        """BallPredTracker's ball-only rollout of every arena's ball (BallPredTracker.cpp:80-88):
+        [num_arenas, len(slice_ticks)] ball states after each slice's tick count.  With
+        to_host False the slices stay in the device buffer RSB_BUF_BALL_PRED and None is
+        returned (ordered on `stream`, not synchronised)."""
+        t = np.ascontiguousarray(slice_ticks, np.int32)
+        if not to_host:
+            self._check(self.lib.rsb_predict_ball(self._h, _ptr(t), len(t), None, 0, C.c_void_p(stream or 0)))
+            return None
+        out = np.zeros((self.num_arenas, len(t)), BALL_DTYPE)
+        self._check(self.lib.rsb_predict_ball(self._h, _ptr(t), len(t), _ptr(out), out.size, C.c_void_p(stream or 0)))
         return out
 
     def set_balls(self, balls: np.ndarray):

@@ -82,7 +82,8 @@ enum {
     RSB_BUF_TERMINALS = 3,  /* uint8 [num_arenas]: RLGymCPP TerminalType: 0 none, 1 normal
                                (goal), 2 truncated (no touch / episode tick limit) */
     RSB_BUF_CONTROLS = 4,   /* rsb_controls [num_cars] */
-    RSB_BUF_ACTIONS = 5     /* int32 [num_cars] */
+    RSB_BUF_ACTIONS = 5,    /* int32 [num_cars] */
+    RSB_BUF_BALL_PRED = 6   /* rsb_ball_state [num_arenas][n_slices] of the last rsb_predict_ball */
 };
 
 /* Arena-narrowphase mode. */
@@ -320,6 +321,20 @@ rsb_status rsb_set_ball_at(rsb_handle* h, int32_t arena, const rsb_ball_state* i
 rsb_status rsb_get_pads_at(rsb_handle* h, int32_t arena, rsb_pad_state* out);
 rsb_status rsb_set_pads_at(rsb_handle* h, int32_t arena, const rsb_pad_state* in);
 rsb_status rsb_get_arena_info_at(rsb_handle* h, int32_t arena, rsb_arena_info* out);
+
+/* Ball prediction: BallPredTracker::ForceUpdateAllPred (RocketSim src/Sim/BallPredTracker/
+ * BallPredTracker.cpp:80-88), the ball-only rollout that VantaObs reads at 1, 2 and 3 s
+ * (RocketSimCudaObs.cuh:92-112), for every arena in one launch.  Each arena's ball goes through
+ * GetState / SetState into a world of its own with no cars, which advances one tick at a time
+ * with the batch's physics; out[a * n_slices + k] is the ball after slice_ticks[k] ticks
+ * (1..8 slices, rising, at most 4096 ticks).  The arenas are only read.  With out non-null the
+ * slices are copied to it (out_count = num_arenas * n_slices) and the stream is synchronised;
+ * with out null they stay on the device (rsb_device_ptr, RSB_BUF_BALL_PRED).  Allocates its
+ * device buffer on the first call of a given size. */
+#define RSB_MAX_PRED_SLICES 8
+#define RSB_MAX_PRED_TICKS 4096
+rsb_status rsb_predict_ball(rsb_handle* h, const int32_t* slice_ticks, int32_t n_slices, rsb_ball_state* out,
+                            size_t out_count, void* stream);
 
 /* One candidate launch configuration of the step kernel and its measured time. */
 typedef struct rsb_tune_entry {

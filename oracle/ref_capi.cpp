@@ -66,6 +66,8 @@ struct rsb_handle {
     std::vector<rsb_controls> lut;
     std::vector<rsb_controls> controls;
     std::vector<int32_t> episodeTicks;
+    MutatorConfig mut = MutatorConfig(GameMode::SOCCAR);
+    std::vector<Arena*> predArenas;  // ball-only arenas of the ball prediction (BallPredTracker)
     int32_t numCars = 0;
     int32_t threads = 1;
     std::string err;
@@ -307,6 +309,7 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     h->numCars = h->carOffset.back();
     MutatorConfig mut(GameMode::SOCCAR);
     if (cfg->mutators) mut = toMutators(*cfg->mutators);
+    h->mut = mut;
     h->arenas.resize(cfg->num_arenas);
     h->cars.resize(cfg->num_arenas);
     for (int a = 0; a < cfg->num_arenas; a++) {
@@ -332,6 +335,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     if (!h) return RSB_ERR_INVALID;
     freeEnv(h);
     for (Arena* a : h->arenas) delete a;
+    for (Arena* a : h->predArenas) delete a;
     delete h;
     return RSB_OK;
 }
@@ -410,17 +414,54 @@ rsb_status rsb_set_cars(rsb_handle* h, const rsb_car_state* in, int32_t n) {
     return RSB_OK;
 }
 
+static rsb_ball_state ballOut(const BallState& s) {
+    rsb_ball_state o{};
+    o.pos = fromVec(s.pos);
+    o.rot.forward = fromVec(s.rotMat.forward);
+    o.rot.right = fromVec(s.rotMat.right);
+    o.rot.up = fromVec(s.rotMat.up);
+    o.vel = fromVec(s.vel);
+    o.ang_vel = fromVec(s.angVel);
+    return o;
+}
+
+// BallPredTracker (BallPredTracker.cpp:3-10, 80-88): one ball-only arena per arena, made once
+// with the batch's mutators; each prediction sets the arena's ball into it and steps one tick
+// at a time, recording the ball after each slice's tick count.
+rsb_status rsb_predict_ball(rsb_handle* h, const int32_t* slice_ticks, int32_t n_slices, rsb_ball_state* out,
+                            size_t out_count, void*) {
+    if (!h || !slice_ticks || n_slices < 1 || n_slices > RSB_MAX_PRED_SLICES)
+        return fail(h, RSB_ERR_INVALID, "rsb_predict_ball: 1..8 slice ticks are required");
+    for (int k = 0; k < n_slices; k++) {
+        const int32_t prev = k ? slice_ticks[k - 1] : 0;
+        if (slice_ticks[k] <= prev || slice_ticks[k] > RSB_MAX_PRED_TICKS)
+            return fail(h, RSB_ERR_INVALID, "rsb_predict_ball: slice ticks must rise, from 1 to 4096");
+    }
+    const size_t n = h->arenas.size();
+    if (!out || out_count != n * (size_t)n_slices)
+        return fail(h, RSB_ERR_INVALID, "rsb_predict_ball: the oracle needs a host out of num_arenas * n_slices");
+    if (h->predArenas.empty()) {
+        for (size_t a = 0; a < n; a++) {
+            Arena* p = Arena::Create(GameMode::SOCCAR);
+            p->SetMutatorConfig(h->mut);
+            h->predArenas.push_back(p);
+        }
+    }
+    forArenas(h, [&](int a) {
+        Arena* p = h->predArenas[a];
+        p->ball->SetState(h->arenas[a]->ball->GetState());
+        int t = 0;
+        for (int k = 0; k < n_slices; k++) {
+            for (; t < slice_ticks[k]; t++) p->Step(1);
+            out[(size_t)a * n_slices + k] = ballOut(p->ball->GetState());
+        }
+    });
+    return RSB_OK;
+}
+
 rsb_status rsb_get_balls(rsb_handle* h, rsb_ball_state* out, int32_t n) {
     if (!h || !out || n != (int32_t)h->arenas.size()) return fail(h, RSB_ERR_INVALID, "ball count must equal num_arenas");
-    for (int a = 0; a < n; a++) {
-        BallState s = h->arenas[a]->ball->GetState();
-        out[a].pos = fromVec(s.pos);
-        out[a].rot.forward = fromVec(s.rotMat.forward);
-        out[a].rot.right = fromVec(s.rotMat.right);
-        out[a].rot.up = fromVec(s.rotMat.up);
-        out[a].vel = fromVec(s.vel);
-        out[a].ang_vel = fromVec(s.angVel);
-    }
+    for (int a = 0; a < n; a++) out[a] = ballOut(h->arenas[a]->ball->GetState());
     return RSB_OK;
 }
 

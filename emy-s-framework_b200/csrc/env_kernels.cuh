@@ -517,7 +517,7 @@ __global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, 
             } else {
                 // within 150-300 uu (horizontally) of the anchor
                 const float r = g.uni(150.f, 300.f), t = g.uni(-PI, PI);
-                pos = V3{anchor.x + r * cosf(t), anchor.y + r * sinf(t), 0.f};
+                pos = V3{anchor.x + r * rsCosf(t), anchor.y + r * rsSinf(t), 0.f};
                 pos.z = air ? fminf(fmaxf(anchor.z + g.uni(-300.f, 300.f), 150.f), 1900.f) : CAR_SPAWN_REST_Z;
             }
             V3 to = anchor - pos;
@@ -525,7 +525,7 @@ __global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, 
             V3 dir = rsNormalized(to);
             if (dir == v3zero()) dir = V3{1.f, 0.f, 0.f};
             const V3 vel = dir * g.uni(1500.f, 2300.f);
-            const float yaw = atan2f(dir.y, dir.x);
+            const float yaw = rsAtan2f(dir.y, dir.x);
             if (air && free) pitch = g.uni(-PI / 4, PI / 4);
             resetCar(E, a, s, pos, angleRot(yaw, pitch, roll), vel, v3zero(), g.uni(0.f, 100.f));
             prev = pos;

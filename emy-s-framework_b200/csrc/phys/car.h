@@ -342,7 +342,6 @@ RSB_HD void carRespawn(World& W, int ci, int pick) {
     // Angle(yaw, 0, 0).ToRotMat() = setEulerYPR(yaw, -0, -0) = setEulerZYX(-0, -0, yaw)
     M3 rot = m3fromEulerZYX(-0.f, -0.f, yaw);
     carSetSpawnState(W, ci, pos, rot, W.P->car.spawnBoost);
-    refreshCastBox(W, 1 + ci);  // the later wheel rays of this tick see the car at its spawn
 }
 
 // Car::_UpdateWheels (Car.cpp:323-461)
@@ -518,10 +517,10 @@ RSB_HD void updateAutoFlip(World& W, int ci, float dt, bool jumpPressed) {
     if (jumpPressed && cflag(c, CF_WORLD_CONTACT) && c.worldContactNormal.z > CAR_AUTOFLIP_NORMZ_THRESH) {
         // Angle::FromRotMat -> btMatrix3x3::getEulerYPR; roll is negated
         const M3& m = c.rotMat;
-        float rollB = atan2f(m.r[2].y, m.r[2].z);
+        float rollB = rsAtan2f(m.r[2].y, m.r[2].z);
         float sp = -m.r[2].x;
         sp = sp < -1.f ? -1.f : (sp > 1.f ? 1.f : sp);
-        float pitchB = asinf(sp);
+        float pitchB = rsAsinf(sp);
         if (fabsf(pitchB) == kHalfPi) {
             if (rollB > 0) rollB -= kPi;
             else rollB += kPi;
@@ -590,8 +589,8 @@ RSB_HD void updateDoubleJumpOrFlip(World& W, int ci, float dt, bool jumpPressed,
                         iv.y *= ((FLIP_SIDE_IMPULSE_MAX_SPEED_SCALE - 1) * fwdRatio) + 1.f;
                         if (back) iv.x *= FLIP_BACKWARD_IMPULSE_SCALE_X;
                         V3 fd = c.rotMat.col(0);
-                        float ang = atan2f(fd.y, fd.x);
-                        V3 xDir{cosf(ang), -sinf(ang), 0.f}, yDir{sinf(ang), cosf(ang), 0.f};
+                        float ang = rsAtan2f(fd.y, fd.x);
+                        V3 xDir{rsCosf(ang), -rsSinf(ang), 0.f}, yDir{rsSinf(ang), rsCosf(ang), 0.f};
                         V3 dv{dot(iv, xDir), dot(iv, yDir), 0.f};
                         rbCentralImpulse(cb, (dv * kUuToBt) * CAR_MASS_BT);
                     }

@@ -139,7 +139,7 @@ RSB_HD void nearestPointInLineSegment(V3 point, V3 l0, V3 l1, V3& nearest) {
 }
 
 RSB_HD float edgeAngle(V3 edgeA, V3 normalA, V3 normalB) {
-    return atan2f(dot(normalB, edgeA), dot(normalB, normalA));
+    return rsAtan2f(dot(normalB, edgeA), dot(normalB, normalA));
 }
 
 RSB_HD bool clampNormal(V3 edge, V3 triNormalOrg, V3 localNormal, float corrected, V3& clamped) {

@@ -3,16 +3,15 @@
 // The reference simulator runs Bullet 3.24 with its x86 SSE code paths
 // (LinearMath/btVector3.h, btMatrix3x3.h, btQuaternion.h, btTransform.h).  The
 // routines below evaluate the same expressions with the same association order,
-// so that single-precision results track the reference as closely as IEEE
-// arithmetic allows.  Two deliberate differences: normalisation starts its
-// Newton step from an exact reciprocal square root (the reference starts from
-// the CPU's 12-bit rsqrt estimate), and transcendental functions come from the
-// platform's math library.  Both differ from the reference by a few ulp.
+// so that single-precision results equal the reference's: normalisation starts its
+// Newton step from the CPU's rsqrtss estimate and sin / cos / atan2 / asin return
+// the reference C library's bits (refmath.h).
 //
 // Conventions follow Bullet: a Mat3 is stored as three rows; `m * v` is three row
 // dot products; `v * m` (tmul) is the transposed product.
 #pragma once
 #include "hd.h"
+#include "refmath.h"
 
 namespace rsb {
 
@@ -58,10 +57,11 @@ RSB_HD V3 vabs(V3 a) { return V3{fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
 RSB_HD V3 vmin(V3 a, V3 b) { return V3{a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z}; }
 RSB_HD V3 vmax(V3 a, V3 b) { return V3{a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z}; }
 
-// btVector3::normalize (SSE path): one Newton-Raphson step on 1/sqrt(|v|^2).
+// btVector3::normalize (SSE path): one Newton-Raphson step on 1/sqrt(|v|^2) from the
+// rsqrtss estimate.
 RSB_HD V3 normalized(V3 a) {
     float l2 = length2(a);
-    float y0 = 1.f / fsqrt(l2);
+    float y0 = rsqrtEstimate(l2);
     float vd = l2 * 0.5f;
     vd = vd * y0;
     vd = vd * y0;
@@ -184,8 +184,8 @@ RSB_HD Quat qsafeNormalized(Quat q) {
 // btQuaternion(axis, angle)
 RSB_HD Quat qaxisAngle(V3 axis, float angle) {
     float d = length(axis);
-    float s = sinf(angle * 0.5f) / d;
-    return Quat{axis.x * s, axis.y * s, axis.z * s, cosf(angle * 0.5f)};
+    float s = rsSinf(angle * 0.5f) / d;
+    return Quat{axis.x * s, axis.y * s, axis.z * s, rsCosf(angle * 0.5f)};
 }
 // quatRotate(rotation, v)
 RSB_HD V3 quatRotate(Quat r, V3 v) {
@@ -242,8 +242,8 @@ RSB_HD Quat quatFromM3(const M3& m) {
 
 // btMatrix3x3::setEulerZYX(eulerX, eulerY, eulerZ)
 RSB_HD M3 m3fromEulerZYX(float ex, float ey, float ez) {
-    float ci = cosf(ex), cj = cosf(ey), ch = cosf(ez);
-    float si = sinf(ex), sj = sinf(ey), sh = sinf(ez);
+    float ci = rsCosf(ex), cj = rsCosf(ey), ch = rsCosf(ez);
+    float si = rsSinf(ex), sj = rsSinf(ey), sh = rsSinf(ez);
     float cc = ci * ch, cs = ci * sh, sc = si * ch, ss = si * sh;
     return m3(cj * ch, sj * sc - cs, sj * cc + ss,
               cj * sh, sj * ss + cc, sj * cs - sc,
@@ -332,9 +332,9 @@ RSB_HD Xf integrateTransform(const Xf& cur, V3 linvel, V3 angvel, float dt) {
     if (ang < 0.001f) {
         axis = angvel * (0.5f * dt - (dt * dt * dt) * (0.020833333333f) * ang * ang);
     } else {
-        axis = angvel * (sinf(0.5f * ang * dt) / ang);
+        axis = angvel * (rsSinf(0.5f * ang * dt) / ang);
     }
-    Quat dorn = Quat{axis.x, axis.y, axis.z, cosf(ang * dt * 0.5f)};
+    Quat dorn = Quat{axis.x, axis.y, axis.z, rsCosf(ang * dt * 0.5f)};
     Quat orn0 = quatFromM3(cur.b);
     Quat pred = qmul(dorn, orn0);
     pred = qsafeNormalized(pred);

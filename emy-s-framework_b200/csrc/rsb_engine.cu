@@ -13,6 +13,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -54,6 +55,11 @@ struct StaticCache {
     std::mutex mu;
     std::map<std::string, std::shared_ptr<ArenaStaticHost>> host;
     std::map<std::pair<int, std::string>, std::shared_ptr<DevStatic>> dev;
+    // rsqrtss table of the host CPU, sampled once; rsqrtExact is false when the CPU's
+    // estimate is not a function of exponent parity and 12 mantissa bits
+    bool rsqrtSampled = false, rsqrtExact = false;
+    uint32_t rsqrtTable[kRsqrtTableSize];
+    std::set<int> rsqrtDevices;  // devices whose g_rsqrtTable holds rsqrtTable
 };
 StaticCache& cache() {
     static StaticCache c;
@@ -379,6 +385,22 @@ __global__ void expandActionsKernel(const int32_t* idx, const rsb_controls* lut,
     out[i] = lut[k];
 }
 
+// The restated float functions of phys/refmath.h on n inputs (rsb_eval_refmath).
+__global__ void refMathKernel(int fn, const float* x, const float* y, float* out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = x[i];
+    float r;
+    switch (fn) {
+        case RSB_MATH_RSQRT_EST: r = rsqrtEstimate(v); break;
+        case RSB_MATH_SIN: r = rsSinf(v); break;
+        case RSB_MATH_COS: r = rsCosf(v); break;
+        case RSB_MATH_ASIN: r = rsAsinf(v); break;
+        default: r = rsAtan2f(v, y[i]); break;
+    }
+    out[i] = r;
+}
+
 // ------------------------------------------------------------------ host helpers
 
 static rsb_status download(rsb_handle* h, const uint32_t* d, std::vector<uint32_t>& host, size_t words) {
@@ -559,6 +581,14 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
                 return fail(nullptr, RSB_ERR_CUDA, "uploading arena meshes failed");
             D->view = deviceView(*H, D->nodes, D->subs, D->triVerts, D->triInfo, D->bpCells, D->occ, D->voxOff,
                                  D->voxList);
+            // the host CPU's rsqrtss estimate, which btVector3::normalize starts from
+            if (!c.rsqrtSampled) {
+                c.rsqrtExact = sampleRsqrtTable(c.rsqrtTable);
+                c.rsqrtSampled = true;
+            }
+            if (cudaMemcpyToSymbol(g_rsqrtTable, c.rsqrtTable, sizeof(c.rsqrtTable)) != cudaSuccess)
+                return fail(nullptr, RSB_ERR_CUDA, "uploading the rsqrt estimate table failed");
+            c.rsqrtDevices.insert(h->device);
             c.dev[key] = D;
             h->stat = D;
         }
@@ -787,6 +817,36 @@ rsb_status rsb_set_step_config(rsb_handle* h, const rsb_tune_entry* cfg) {
                 return RSB_OK;
             }
     return fail(h, RSB_ERR_INVALID, "rsb_set_step_config: no such launch configuration");
+}
+
+rsb_status rsb_eval_refmath(int32_t fn, const float* x, const float* y, float* out, int64_t n, int32_t device) {
+    rsb_handle* h = nullptr;
+    if (fn < RSB_MATH_RSQRT_EST || fn > RSB_MATH_ATAN2 || !x || !out || n < 0 || (fn == RSB_MATH_ATAN2 && !y))
+        return fail(h, RSB_ERR_INVALID, "bad function, pointer or count");
+    if (n == 0) return RSB_OK;
+    if (fn == RSB_MATH_RSQRT_EST) {
+        StaticCache& c = cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        if (!c.rsqrtDevices.count(device))
+            return fail(h, RSB_ERR_STATE, "no rsb_create on this device yet: the rsqrt table is not loaded");
+    }
+    RSB_CUDA(cudaSetDevice(device));
+    const size_t bytes = (size_t)n * 4;
+    float *dx = nullptr, *dy = nullptr, *dout = nullptr;
+    auto release = [&] { cudaFree(dx); cudaFree(dy); cudaFree(dout); };
+    cudaError_t e = cudaMalloc(&dx, bytes);
+    if (e == cudaSuccess && y) e = cudaMalloc(&dy, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && y) e = cudaMemcpy(dy, y, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        refMathKernel<<<(unsigned)((n + 255) / 256), 256>>>(fn, dx, dy, dout, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, bytes, cudaMemcpyDeviceToHost);
+    release();
+    if (e != cudaSuccess) return cudaFail(h, "rsb_eval_refmath", e);
+    return RSB_OK;
 }
 
 rsb_status rsb_sync(rsb_handle* h) {

@@ -33,6 +33,7 @@ RSB_MAX_PRED_TICKS = 4096
 RSB_CULL_EXACT, RSB_CULL_LEARNED, RSB_CULL_LEARNED_AUDIT = 0, 1, 2
 RSB_CULLER_PARAMS = 4481
 RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT = 0, 1, 2
+RSB_MATH_RSQRT_EST, RSB_MATH_SIN, RSB_MATH_COS, RSB_MATH_ASIN, RSB_MATH_ATAN2 = range(5)
 RSB_ARENA_NONFINITE, RSB_ARENA_ROW_OVERFLOW, RSB_ARENA_BVH_OVERFLOW, RSB_ARENA_CULL_MISS, RSB_ARENA_EPA_OVERFLOW = (
     1, 2, 4, 8, 16)
 
@@ -249,6 +250,7 @@ _SIGS = {
     "rsb_sync": [_P],
     "rsb_stats_get": [_P, C.POINTER(Stats)],
     "rsb_last_error": [_P, C.c_char_p, C.c_size_t],
+    "rsb_eval_refmath": [C.c_int32, _P, _P, _P, C.c_int64, C.c_int32],
 }
 
 #: every symbol include/rsb.h declares (checked by the ABI tests)
@@ -348,6 +350,18 @@ def compute_gae(lib: C.CDLL, rews, terminals, val_preds, trunc_val_preds=None, p
     if st != 0:
         raise RsbError(st, _global_error(lib))
     return adv, tgt, ret, float(clip[0])
+
+
+def eval_refmath(lib: C.CDLL, fn: int, x, y=None, device: int = 0) -> np.ndarray:
+    """rsb_eval_refmath on numpy arrays (float32): the device's restated rsqrtss / sinf / cosf /
+    asinf / atan2f(x, y)."""
+    x = np.ascontiguousarray(x, np.float32)
+    yy = None if y is None else np.ascontiguousarray(y, np.float32)
+    out = np.empty_like(x)
+    st = lib.rsb_eval_refmath(fn, _ptr(x), _ptr(yy) if yy is not None else None, _ptr(out), len(x), device)
+    if st != 0:
+        raise RsbError(st, _global_error(lib))
+    return out
 
 
 def _global_error(lib: C.CDLL) -> str:

@@ -505,6 +505,16 @@ rsb_status rsb_compute_gae_host(const float* rews, const int8_t* terminals, cons
                                 float* advantages, float* target_values, float* returns,
                                 float* rew_clip_portion, int32_t T, const rsb_gae_params* params);
 
+/* Diagnostic (no counterpart in the reference): evaluates on device `device` the float
+ * functions whose bits the simulation takes from the reference's CPU build, for n inputs:
+ *   RSB_MATH_RSQRT_EST  x86 rsqrtss estimate of x (the table sampled from this host's CPU at
+ *                       the first rsb_create on the device; RSB_ERR_STATE before that)
+ *   RSB_MATH_SIN/COS/ASIN  sinf / cosf / asinf of x as the host C library returns them
+ *   RSB_MATH_ATAN2      atan2f(x, y) (x is the y-coordinate, as in the C function)
+ * y may be NULL except for RSB_MATH_ATAN2.  Host buffers; synchronous. */
+enum { RSB_MATH_RSQRT_EST = 0, RSB_MATH_SIN = 1, RSB_MATH_COS = 2, RSB_MATH_ASIN = 3, RSB_MATH_ATAN2 = 4 };
+rsb_status rsb_eval_refmath(int32_t fn, const float* x, const float* y, float* out, int64_t n, int32_t device);
+
 rsb_status rsb_sync(rsb_handle* h);
 rsb_status rsb_stats_get(rsb_handle* h, rsb_stats* out);
 /* Copies the last error message (NUL-terminated, truncated to n). Safe with h == NULL

@@ -32,7 +32,10 @@
 #include "RLGymCPP/TerminalConditions/GoalScoreCondition.h"
 #include "RLGymCPP/TerminalConditions/NoTouchCondition.h"
 
+#include <xmmintrin.h>
+
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -814,6 +817,23 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t, rsb_tune_entry*, int32_t, int32_
     return RSB_OK;
 }
 
+// The reference's own values of the functions the engine restates: the CPU's rsqrtss and the
+// C library's sinf / cosf / asinf / atan2f, evaluated here on the host.
+rsb_status rsb_eval_refmath(int32_t fn, const float* x, const float* y, float* out, int64_t n, int32_t) {
+    if (fn < RSB_MATH_RSQRT_EST || fn > RSB_MATH_ATAN2 || !x || !out || n < 0 || (fn == RSB_MATH_ATAN2 && !y))
+        return fail(nullptr, RSB_ERR_INVALID, "bad function, pointer or count");
+    for (int64_t i = 0; i < n; i++) {
+        switch (fn) {
+            case RSB_MATH_RSQRT_EST: out[i] = _mm_cvtss_f32(_mm_rsqrt_ss(_mm_set_ss(x[i]))); break;
+            case RSB_MATH_SIN: out[i] = sinf(x[i]); break;
+            case RSB_MATH_COS: out[i] = cosf(x[i]); break;
+            case RSB_MATH_ASIN: out[i] = asinf(x[i]); break;
+            default: out[i] = atan2f(x[i], y[i]); break;
+        }
+    }
+    return RSB_OK;
+}
+
 // Oracle-only helpers (not part of include/rsb.h).
 //
 // rsbref_car_order: the order in which the reference visits the cars of arena `a` on
@@ -827,6 +847,29 @@ int32_t rsbref_car_order(rsb_handle* h, int32_t a, int32_t* order) {
             if (h->cars[a][s] == c) order[k++] = (int32_t)s;
     }
     return k;
+}
+// rsbref_wheel_info: the raycast result of wheel w of car slot s in arena a, as the last
+// tick's pre-tick left it (btWheelInfo::RaycastInfo): hard point (3), direction (3), contact
+// point (3), contact normal (3), suspension length, in contact (1/0), ground object kind
+// (-1 none, 0 static, 1 ball, 2 car), all in Bullet units.  Writes 16 floats.
+int32_t rsbref_wheel_info(rsb_handle* h, int32_t a, int32_t s, int32_t w, float* out) {
+    if (!h || a < 0 || a >= (int32_t)h->arenas.size() || s < 0 || s >= (int32_t)h->cars[a].size() || w < 0 ||
+        w > 3 || !out)
+        return -1;
+    const btWheelInfo::RaycastInfo& r = h->cars[a][s]->_bulletVehicle.m_wheelInfo[w].m_raycastInfo;
+    const btVector3* v[4] = {&r.m_hardPointWS, &r.m_wheelDirectionWS, &r.m_contactPointWS, &r.m_contactNormalWS};
+    for (int k = 0; k < 4; k++)
+        for (int c = 0; c < 3; c++) out[3 * k + c] = (*v[k])[c];
+    out[12] = r.m_suspensionLength;
+    out[13] = r.m_isInContact ? 1.f : 0.f;
+    float kind = -1.f;
+    if (r.m_groundObject) {
+        const btCollisionObject* o = (const btCollisionObject*)r.m_groundObject;
+        kind = o->isStaticObject() ? 0.f : (o->getCollisionShape()->getShapeType() == SPHERE_SHAPE_PROXYTYPE ? 1.f : 2.f);
+    }
+    out[14] = kind;
+    out[15] = 0.f;
+    return 0;
 }
 // rsbref_car_ptr: the reference Car object of slot s in arena a (debug probes)
 void* rsbref_car_ptr(rsb_handle* h, int32_t a, int32_t s) {

@@ -8,7 +8,8 @@
 //                    (CommonRewards.h:33-98, ZeroSumReward.cpp:3-31, GoalScoreCondition.h,
 //                    NoTouchCondition.h, EnvSet.cpp:184-254)
 //   resetKernel .... seeded arena resets: kickoff (Arena::ResetToRandomKickoff
-//                    Arena.cpp:112-216), random state (RandomState.cpp:9-60), high-contact
+//                    Arena.cpp:112-216), random state (RandomState.cpp:9-60), the reference
+//                    batch's curriculum (RocketSimCudaApi.cuh:203-442), high-contact
 //
 // Player order.  EnvSet walks the players of an arena in Arena::_cars order, which the
 // physics kernel takes to be reverse creation order (the order libstdc++'s unordered_set
@@ -405,7 +406,8 @@ RSB_D void putCarF(const EnvView& E, int a, int s, int w, float v) { putCarW(E, 
 // Car::SetState of a default CarState with the given placement (Car.cpp:23-36,
 // Car.h:15-100): the transform, the velocities and every CarState field are replaced;
 // the broadphase registration and the vehicle's wheel values are kept.
-RSB_D void resetCar(const EnvView& E, int a, int s, V3 posUu, const M3& rot, V3 velUu, V3 ang, float boost) {
+RSB_D void resetCarFlags(const EnvView& E, int a, int s, V3 posUu, const M3& rot, V3 velUu, V3 ang, float boost,
+                         uint32_t flags) {
     // the team and the body's contact-response flag survive Car::SetState
     const uint32_t team = carW(E, a, s, CW_FLAGS) & (CF_TEAM_ORANGE | CF_NO_RESPONSE);
     const V3 p = posUu * kUuToBt, v = velUu * kUuToBt;
@@ -421,7 +423,7 @@ RSB_D void resetCar(const EnvView& E, int a, int s, V3 posUu, const M3& rot, V3 
     // CarState words (boost .. lastCtlBits): defaults, then the placement
     for (int w = CW_STATE0; w < CW_STATE1; w++) putCarW(E, a, s, w, 0u);
     putCarF(E, a, s, CW_BOOST, boost);
-    putCarW(E, a, s, CW_FLAGS, CF_ON_GROUND | team);
+    putCarW(E, a, s, CW_FLAGS, flags | team);
     for (int k = 0; k < 2; k++) {
         putCarW(E, a, s, CW_HIT + k, 0xffffffffu);
         putCarW(E, a, s, CW_HITX + k, 0xffffffffu);
@@ -433,6 +435,17 @@ RSB_D void resetCar(const EnvView& E, int a, int s, V3 posUu, const M3& rot, V3 
     }
 }
 
+RSB_D void resetCar(const EnvView& E, int a, int s, V3 posUu, const M3& rot, V3 velUu, V3 ang, float boost) {
+    resetCarFlags(E, a, s, posUu, rot, velUu, ang, boost, CF_ON_GROUND);
+}
+
+// Weights of the curriculum reset (RocketSimCudaBatch::SetResetCurriculum) and the no-touch
+// timeout whose timer it staggers.
+struct ResetCurriculum {
+    float w[4];  // kickoff, fuzzed kickoff, aerial, ball chase
+    float noTouchTimeout;
+};
+
 RSB_D M3 rowsToM3(const float* r) { return m3(r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8]); }
 
 // Angle(yaw, pitch, roll).ToRotMat() = btMatrix3x3::setEulerYPR(yaw, -pitch, -roll)
@@ -441,8 +454,8 @@ RSB_D M3 angleRot(float yaw, float pitch, float roll) { return m3fromEulerZYX(-r
 
 // Arena i of the list `idx` (every arena when idx is null; with `onlyDone`, only the
 // arenas whose terminal flag is set).
-__global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, uint64_t seed, int mode,
-                            bool onlyDone) {
+__global__ void resetKernel(EnvView E, EnvTables Tb, ResetCurriculum Cu, const int32_t* idx, int n, uint64_t seed,
+                            int mode, bool onlyDone) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int a = idx ? idx[i] : i;
@@ -450,6 +463,15 @@ __global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, 
     const int T = E.teamSize[a], M = 2 * T, base = E.carOffset[a];
     ResetRng g{seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(a + 1)), 0};
     constexpr float PI = 3.14159265358979323846f;
+    // curriculum: 0 kickoff, 1 fuzzed kickoff, 2 aerial, 3 ball chase, drawn by weight
+    // (RocketSimCudaBatch::ResetArena, RocketSimCudaApi.cuh:216-245)
+    int cur = -1;
+    if (mode == RSB_RESET_CURRICULUM) {
+        const float tot = Cu.w[0] + Cu.w[1] + Cu.w[2] + Cu.w[3];
+        const float r = g.uni(0.f, 1.f) * tot;
+        cur = r < Cu.w[0] ? 0 : (r < Cu.w[0] + Cu.w[1] ? 1 : (r < Cu.w[0] + Cu.w[1] + Cu.w[2] ? 2 : 3));
+    }
+    auto sgn = [&](float amp) { return g.uni(-amp, amp); };
 
     // kickoff layout (always applied first, as RandomState does): a shuffled spawn per
     // kickoff rank, rank i of each team taking the i-th car in Arena::_cars order
@@ -464,6 +486,10 @@ __global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, 
             const int s = team * T + (T - 1 - r);
             V3 pos{Tb.kickX[sp], Tb.kickY[sp], CAR_SPAWN_REST_Z};
             if (team) pos = pos * V3{-1.f, -1.f, 1.f};
+            if (cur == 1) {  // fuzzed kickoff: the slot and yaw kept, the position moved a little
+                pos.x += sgn(40.f);
+                pos.y += sgn(40.f);
+            }
             resetCar(E, a, s, pos, rowsToM3(Tb.kickRot[team][sp]), v3zero(), v3zero(), BOOST_SPAWN_AMOUNT);
         }
     }
@@ -488,6 +514,46 @@ __global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, 
                 ang = v3zero();
             }
             resetCar(E, a, s, pos, angleRot(yaw, pitch, roll), vel, ang, g.uni(0.f, 100.f));
+        }
+    } else if (cur == 1) {
+        // fuzzed kickoff: the ball a little off the spot with a mild velocity
+        ballPos = V3{sgn(180.f), sgn(220.f), BALL_REST_Z};
+        ballVel = V3{sgn(90.f), sgn(90.f), sgn(35.f)};
+    } else if (cur == 2) {
+        // aerial: the ball raised near midfield, one car below it moving toward it
+        ballPos = V3{sgn(1400.f), sgn(1600.f), 420.f + g.uni(0.f, 360.f)};
+        ballVel = V3{sgn(100.f), sgn(100.f), sgn(50.f)};
+        const int s = (int)(g.uni(0.f, 1.f) * (float)M) % M;
+        V3 d{sgn(1.f), sgn(1.f), 0.f};
+        float len = sqrtf(d.x * d.x + d.y * d.y);
+        if (len < 1e-3f) { d = V3{1.f, 0.f, 0.f}; len = 1.f; }
+        d = V3{d.x / len, d.y / len, 0.f};
+        const float dist = 180.f + g.uni(0.f, 160.f);
+        V3 pos{ballPos.x - d.x * dist, ballPos.y - d.y * dist, ballPos.z - (40.f + g.uni(0.f, 120.f))};
+        if (pos.z < CAR_SPAWN_REST_Z) pos.z = CAR_SPAWN_REST_Z + 80.f;
+        const float yaw = rsAtan2f(ballPos.y - pos.y, ballPos.x - pos.x);
+        const float spd = 500.f + g.uni(0.f, 400.f);
+        const V3 vel{d.x * spd, d.y * spd, 80.f + g.uni(0.f, 120.f)};
+        const bool jumped = g.uni(0.f, 1.f) < 0.55f;
+        resetCarFlags(E, a, s, pos, angleRot(yaw, 0.f, 0.f), vel, v3zero(), 55.f + g.uni(0.f, 45.f),
+                      jumped ? CF_HAS_JUMPED : 0u);
+    } else if (cur == 3) {
+        // ball chase: the ball in play on the ground, every car near it on the ground facing it
+        ballPos = V3{sgn(1900.f), sgn(2200.f), BALL_REST_Z};
+        ballVel = V3{sgn(500.f), sgn(500.f), sgn(80.f)};
+        for (int s = 0; s < M; s++) {
+            V3 d{sgn(1.f), sgn(1.f), 0.f};
+            float len = sqrtf(d.x * d.x + d.y * d.y);
+            if (len < 1e-3f) { d = V3{1.f, 0.f, 0.f}; len = 1.f; }
+            d = V3{d.x / len, d.y / len, 0.f};
+            const float dist = 450.f + g.uni(0.f, 1400.f);
+            V3 pos{fminf(fmaxf(ballPos.x + d.x * dist, -3500.f), 3500.f),
+                   fminf(fmaxf(ballPos.y + d.y * dist, -4500.f), 4500.f), CAR_SPAWN_REST_Z};
+            const float yaw = rsAtan2f(ballPos.y - pos.y, ballPos.x - pos.x);
+            const float spd = g.uni(0.f, 600.f);
+            const float tx = ballPos.x - pos.x, ty = ballPos.y - pos.y, tl = sqrtf(tx * tx + ty * ty);
+            const V3 vel = tl > 1.f ? V3{tx / tl * spd, ty / tl * spd, 0.f} : v3zero();
+            resetCar(E, a, s, pos, angleRot(yaw, 0.f, 0.f), vel, v3zero(), 30.f + g.uni(0.f, 70.f));
         }
     } else if (mode == RSB_RESET_HIGH_CONTACT) {
         // cars within 300 uu of the ball or of another car, 1500-2300 uu/s toward it,
@@ -553,7 +619,10 @@ __global__ void resetKernel(EnvView E, EnvTables Tb, const int32_t* idx, int n, 
     E.arena[(size_t)AW_STATUS * E.N + a] = 0;
     E.arena[(size_t)AW_GOALTEAM * E.N + a] = (uint32_t)-1;
     E.arena[(size_t)AW_TOUCHED * E.N + a] = 0;
-    E.arena[(size_t)AW_NOTOUCH * E.N + a] = 0;
+    // the curriculum staggers the no-touch timers so that arenas reset together do not all
+    // time out on the same step (RocketSimCudaApi.cuh:417-427)
+    E.arena[(size_t)AW_NOTOUCH * E.N + a] =
+        (cur >= 0 && Cu.noTouchTimeout > 0.f) ? __float_as_uint(g.uni(0.f, 1.f) * Cu.noTouchTimeout * 0.9f) : 0u;
     // every reset places the ball inside the field (|y| <= 4000 uu), short of a goal line
     E.arena[(size_t)AW_SCORED * E.N + a] = 0;
     // the new state's players carry default (zero) actions

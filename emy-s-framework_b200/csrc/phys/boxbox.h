@@ -4,6 +4,27 @@
 // reference face and keeps up to four points (cullPoints2 when more survive).
 //
 // Matrices are addressed as the reference's dMatrix3: R[4*row + col] holds basis[row][col].
+//
+// ALTERED SOURCE: this file is not the original Bullet code.  It restates the algorithm of
+// the Bullet 3.24 file named above (ODE's box-box detector, as RocketSim builds it) for a
+// CUDA device and a host build, with its own data layout and naming; the original's notice
+// follows.
+//
+// Box-Box collision detection re-distributed under the ZLib license with permission from Russell L. Smith
+// Original version is from Open Dynamics Engine, Copyright (C) 2001,2002 Russell L. Smith.
+// All rights reserved.  Email: russ@q12.org   Web: www.q12.org
+// Bullet Continuous Collision Detection and Physics Library
+// Bullet is Copyright (c) 2003-2006 Erwin Coumans  https://bulletphysics.org
+//
+// This software is provided 'as-is', without any express or implied warranty.
+// In no event will the authors be held liable for any damages arising from the use of this software.
+// Permission is granted to anyone to use this software for any purpose,
+// including commercial applications, and to alter it and redistribute it freely,
+// subject to the following restrictions:
+//
+// 1. The origin of this software must not be misrepresented; you must not claim that you wrote the original software. If you use this software in a product, an acknowledgment in the product documentation would be appreciated but is not required.
+// 2. Altered source versions must be plainly marked as such, and must not be misrepresented as being the original software.
+// 3. This notice may not be removed or altered from any source distribution.
 #pragma once
 #include "vecmath.h"
 

@@ -12,6 +12,25 @@
 //                        fixed arrays addressed by index, and EPA's recursive horizon walk
 //                        runs on an explicit stack in the same visiting order
 //   subsimplexCast ..... btSubsimplexConvexCast::calcTimeOfImpact (btSubSimplexConvexCast.cpp:31-147)
+//
+// ALTERED SOURCE: this file is not the original Bullet code.  It restates the algorithms of
+// the Bullet 3.24 files named above (as patched in RocketSim) for a CUDA device and a host
+// build, with its own data layout, naming and control flow; the original's notice follows.
+//
+// Bullet Continuous Collision Detection and Physics Library
+// Copyright (c) 2003-2008 Erwin Coumans  https://bulletphysics.org
+//
+// This software is provided 'as-is', without any express or implied warranty.
+// In no event will the authors be held liable for any damages arising from the use of this software.
+// Permission is granted to anyone to use this software for any purpose,
+// including commercial applications, and to alter it and redistribute it freely,
+// subject to the following restrictions:
+//
+// 1. The origin of this software must not be misrepresented; you must not claim that you wrote the original software. If you use this software in a product, an acknowledgment in the product documentation would be appreciated but is not required.
+// 2. Altered source versions must be plainly marked as such, and must not be misrepresented as being the original software.
+// 3. This notice may not be removed or altered from any source distribution.
+//
+// GJK-EPA collision solver by Nathanael Presson, 2008
 #pragma once
 #include "shapes.h"
 

@@ -10,6 +10,23 @@
 //     USE_PATH_COMPRESSION (btSimulationIslandManager.cpp, btUnionFind.h), including
 //     the unstable quickSort of btAlignedObjectArray that fixes manifold order;
 //   - integrateTransforms / updateActivationState.
+//
+// ALTERED SOURCE: this file is not the original Bullet code.  It restates the algorithms of
+// the Bullet 3.24 files named above (as patched in RocketSim) for a CUDA device and a host
+// build, with its own data layout, naming and control flow; the original's notice follows.
+//
+// Bullet Continuous Collision Detection and Physics Library
+// Copyright (c) 2003-2006 Erwin Coumans  https://bulletphysics.org
+//
+// This software is provided 'as-is', without any express or implied warranty.
+// In no event will the authors be held liable for any damages arising from the use of this software.
+// Permission is granted to anyone to use this software for any purpose,
+// including commercial applications, and to alter it and redistribute it freely,
+// subject to the following restrictions:
+//
+// 1. The origin of this software must not be misrepresented; you must not claim that you wrote the original software. If you use this software in a product, an acknowledgment in the product documentation would be appreciated but is not required.
+// 2. Altered source versions must be plainly marked as such, and must not be misrepresented as being the original software.
+// 3. This notice may not be removed or altered from any source distribution.
 #pragma once
 #include "contacts.h"
 #include "solver.h"
@@ -63,7 +80,7 @@ struct World {
 };
 
 // world status bits (per-arena status word)
-enum : uint32_t { WS_NONFINITE = 1u, WS_OVERFLOW = 2u, WS_BVH_OVERFLOW = 4u, WS_CULL_MISS = 8u, WS_EPA_OVERFLOW = 16u };
+enum : uint32_t { WS_NONFINITE = 1u, WS_OVERFLOW = 2u, WS_CULL_MISS = 8u, WS_EPA_OVERFLOW = 16u };  // 4 is reserved (rsb.h)
 
 // Index of the lowest set bit of a non-zero mask.
 RSB_HD int lowestBit(uint32_t m) {
@@ -929,10 +946,15 @@ struct UnionFind {
     }
 };
 
-// btAlignedObjectArray::quickSortInternal on (key, value) pairs, ascending by key
-RSB_HD void quickSortKV(int* key, int* val, int lo, int hi) {
+// btAlignedObjectArray::quickSortInternal on (key, value) pairs, ascending by key.  The
+// ranges waiting on the explicit stack are disjoint and hold at least two elements each, so
+// sorting at most MAX_MANIFOLDS elements never needs more than MAX_MANIFOLDS / 2 of them;
+// should a range not fit, the sort sets WS_OVERFLOW in `status` instead of skipping it
+// silently.
+constexpr int kSortStack = 2 * (MAX_MANIFOLDS / 2);
+RSB_HD void quickSortKV(int* key, int* val, int lo, int hi, uint32_t& status) {
     // explicit stack keeps the device code free of recursion
-    int stack[64];
+    int stack[kSortStack];
     int sp = 0;
     stack[sp++] = lo;
     stack[sp++] = hi;
@@ -952,8 +974,14 @@ RSB_HD void quickSortKV(int* key, int* val, int lo, int hi) {
             }
         } while (i <= j);
         // the reference recurses on (lo, j) first, then (i, hi): push in reverse
-        if (i < h && sp + 2 <= 64) { stack[sp++] = i; stack[sp++] = h; }
-        if (l < j && sp + 2 <= 64) { stack[sp++] = l; stack[sp++] = j; }
+        if (i < h) {
+            if (sp + 2 <= kSortStack) { stack[sp++] = i; stack[sp++] = h; }
+            else status |= WS_OVERFLOW;
+        }
+        if (l < j) {
+            if (sp + 2 <= kSortStack) { stack[sp++] = l; stack[sp++] = j; }
+            else status |= WS_OVERFLOW;
+        }
     }
 }
 
@@ -977,7 +1005,7 @@ RSB_HD void solveIslands(World& W) {
     // sortIslands: element (m_id = find(i), m_sz = collision object index)
     int eid[MAX_BODIES], eobj[MAX_BODIES];
     for (int i = 0; i < W.nb; i++) { eid[i] = uf.find(i); eobj[i] = i; }
-    if (W.nb > 1) quickSortKV(eid, eobj, 0, W.nb - 1);
+    if (W.nb > 1) quickSortKV(eid, eobj, 0, W.nb - 1, W.status);
 
     // buildIslands: sleeping bookkeeping
     for (int s = 0; s < W.nb;) {
@@ -1019,7 +1047,7 @@ RSB_HD void solveIslands(World& W) {
         midx[nim] = i;
         nim++;
     }
-    if (nim > 1) quickSortKV(mkey, midx, 0, nim - 1);
+    if (nim > 1) quickSortKV(mkey, midx, 0, nim - 1, W.status);
 
     // processIslands -> one batched solveGroup
     int bodyList[MAX_BODIES], nbl = 0;

@@ -138,6 +138,7 @@ struct rsb_handle {
     size_t predCap = 0;
     size_t stageWords = 0;
     EnvTables tables{};
+    ResetCurriculum curriculum{{1.f, 0.f, 0.f, 0.f}, 0.f};
     bool hasRewards = false;
     RewardParams rewardParams{};
     std::string err;
@@ -544,6 +545,7 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
         R.zeroSum = r.zero_sum;
         R.episodeMaxTicks = r.episode_max_ticks;
         R.noTouchTimeout = r.no_touch_timeout_s;
+        h->curriculum.noTouchTimeout = r.no_touch_timeout_s;
         R.goalBaseY = h->mut.goal_base_threshold_y;
         R.ballRadius = h->mut.ball_radius;
     }
@@ -1687,13 +1689,14 @@ rsb_status rsb_device_ptr(rsb_handle* h, int32_t which, void** out) {
 
 rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* idx, int32_t n, uint64_t seed, int32_t mode) {
     if (!h || n < 0 || (n > 0 && !idx) || n > h->N) return fail(h, RSB_ERR_INVALID, "bad reset arena list");
-    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_HIGH_CONTACT) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
+    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_CURRICULUM) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
     for (int i = 0; i < n; i++)
         if (idx[i] < 0 || idx[i] >= h->N) return fail(h, RSB_ERR_INVALID, "arena index out of range");
     if (n == 0) return RSB_OK;
     RSB_CUDA(cudaSetDevice(h->device));
     RSB_CUDA(cudaMemcpyAsync(h->dResetIdx, idx, 4 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
-    resetKernel<<<(n + 127) / 128, 128, 0, h->stream>>>(envView(h), h->tables, h->dResetIdx, n, seed, mode, false);
+    resetKernel<<<(n + 127) / 128, 128, 0, h->stream>>>(envView(h), h->tables, h->curriculum, h->dResetIdx, n, seed,
+                                                         mode, false);
     RSB_CUDA(cudaGetLastError());
     RSB_CUDA(cudaStreamSynchronize(h->stream));
     return RSB_OK;
@@ -1701,9 +1704,10 @@ rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* idx, int32_t n, uint64
 
 rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode) {
     if (!h) return RSB_ERR_INVALID;
-    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_HIGH_CONTACT) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
+    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_CURRICULUM) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
     RSB_CUDA(cudaSetDevice(h->device));
-    resetKernel<<<(h->N + 127) / 128, 128, 0, h->stream>>>(envView(h), h->tables, nullptr, h->N, seed, mode, false);
+    resetKernel<<<(h->N + 127) / 128, 128, 0, h->stream>>>(envView(h), h->tables, h->curriculum, nullptr, h->N, seed,
+                                                            mode, false);
     RSB_CUDA(cudaGetLastError());
     RSB_CUDA(cudaStreamSynchronize(h->stream));
     return RSB_OK;
@@ -1711,10 +1715,23 @@ rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode) {
 
 rsb_status rsb_reset_done(rsb_handle* h, uint64_t seed, int32_t mode, void* stream) {
     if (!h) return RSB_ERR_INVALID;
-    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_HIGH_CONTACT) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
+    if (mode < RSB_RESET_KICKOFF || mode > RSB_RESET_CURRICULUM) return fail(h, RSB_ERR_INVALID, "unknown reset mode");
     RSB_CUDA(cudaSetDevice(h->device));
-    resetKernel<<<(h->N + 127) / 128, 128, 0, pick(h, stream)>>>(envView(h), h->tables, nullptr, h->N, seed, mode, true);
+    resetKernel<<<(h->N + 127) / 128, 128, 0, pick(h, stream)>>>(envView(h), h->tables, h->curriculum, nullptr, h->N,
+                                                                  seed, mode, true);
     RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+rsb_status rsb_set_reset_curriculum(rsb_handle* h, float kickoff_w, float fuzzed_w, float aerial_w, float chase_w) {
+    if (!h) return RSB_ERR_INVALID;
+    auto clampW = [](float w) { return (w >= 0.f && w <= 1e6f) ? w : 0.f; };
+    float* w = h->curriculum.w;
+    w[0] = clampW(kickoff_w);
+    w[1] = clampW(fuzzed_w);
+    w[2] = clampW(aerial_w);
+    w[3] = clampW(chase_w);
+    if (w[0] + w[1] + w[2] + w[3] <= 0.f) w[0] = 1.f;
     return RSB_OK;
 }
 

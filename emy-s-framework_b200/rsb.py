@@ -32,7 +32,7 @@ RSB_MAX_PRED_SLICES = 8
 RSB_MAX_PRED_TICKS = 4096
 RSB_CULL_EXACT, RSB_CULL_LEARNED, RSB_CULL_LEARNED_AUDIT = 0, 1, 2
 RSB_CULLER_PARAMS = 4481
-RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT = 0, 1, 2
+RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT, RSB_RESET_CURRICULUM = 0, 1, 2, 3
 RSB_MATH_RSQRT_EST, RSB_MATH_SIN, RSB_MATH_COS, RSB_MATH_ASIN, RSB_MATH_ATAN2 = range(5)
 RSB_ARENA_NONFINITE, RSB_ARENA_ROW_OVERFLOW, RSB_ARENA_BVH_OVERFLOW, RSB_ARENA_CULL_MISS, RSB_ARENA_EPA_OVERFLOW = (
     1, 2, 4, 8, 16)
@@ -251,6 +251,7 @@ _SIGS = {
     "rsb_stats_get": [_P, C.POINTER(Stats)],
     "rsb_last_error": [_P, C.c_char_p, C.c_size_t],
     "rsb_eval_refmath": [C.c_int32, _P, _P, _P, C.c_int64, C.c_int32],
+    "rsb_set_reset_curriculum": [_P, C.c_float, C.c_float, C.c_float, C.c_float],
 }
 
 #: every symbol include/rsb.h declares (checked by the ABI tests)
@@ -512,6 +513,9 @@ class Batch:
     def reset_arenas(self, idx, seed: int, mode: int = RSB_RESET_KICKOFF):
         a = np.ascontiguousarray(idx, np.int32)
         self._check(self.lib.rsb_reset_arenas(self._h, _ptr(a), len(a), seed, mode))
+
+    def set_reset_curriculum(self, kickoff_w: float, fuzzed_w: float, aerial_w: float, chase_w: float = 0.0):
+        self._check(self.lib.rsb_set_reset_curriculum(self._h, kickoff_w, fuzzed_w, aerial_w, chase_w))
 
     def reset_done(self, seed: int, mode: int = RSB_RESET_KICKOFF, stream: int | None = None):
         """Resets the arenas whose terminal flag is set (device-side, stream-ordered)."""

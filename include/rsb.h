@@ -14,6 +14,7 @@
  *                                                          laid out blue first, then orange)
  *   RocketSimCudaBatch::ResetArena      :275               rsb_reset_arenas
  *   RocketSimCudaBatch::ResetAllArenas  :278               rsb_reset_all
+ *   RocketSimCudaBatch::SetResetCurriculum :283            rsb_set_reset_curriculum
  *   RocketSimCudaBatch::UploadDiscreteActionLut :293       rsb_set_action_lut
  *   RocketSimCudaBatch::SetDiscreteActionsFromIndices :297 rsb_set_actions_host
  *   RocketSimCudaBatch::SetDiscreteActionsFromDevice  :300 rsb_set_actions_device
@@ -100,9 +101,13 @@ enum {
     RSB_RESET_KICKOFF = 0,      /* RocketSim Arena::ResetToRandomKickoff layout */
     RSB_RESET_RANDOM_STATE = 1, /* RLGymCPP RandomState(true, true, false): uniform random
                                    cars/ball inside the field, half the cars on the ground */
-    RSB_RESET_HIGH_CONTACT = 2  /* cars within 300 uu of the ball or each other, 1500-2300
+    RSB_RESET_HIGH_CONTACT = 2, /* cars within 300 uu of the ball or each other, 1500-2300
                                    uu/s toward it, half airborne, some on walls / ceiling
                                    (no CPU counterpart in the reference) */
+    RSB_RESET_CURRICULUM = 3    /* per arena, one of kickoff / fuzzed kickoff / aerial / ball
+                                   chase drawn with the weights of rsb_set_reset_curriculum
+                                   (the reference batch's ResetArena, RocketSimCudaApi.cuh:216-442;
+                                   GPU-only: the CPU reference has no curriculum) */
 };
 
 typedef struct rsb_vec3 { float x, y, z; } rsb_vec3;
@@ -174,8 +179,9 @@ typedef struct rsb_arena_info {
 /* Per-arena status bits (rsb_arena_info.status). */
 enum {
     RSB_ARENA_NONFINITE = 1,       /* NaN/Inf appeared in the state; arena should be reset */
-    RSB_ARENA_ROW_OVERFLOW = 2,    /* more solver rows than the fixed pool; extra contacts dropped */
-    RSB_ARENA_BVH_OVERFLOW = 4,    /* BVH traversal stack overflowed; query fell back to a linear scan */
+    RSB_ARENA_ROW_OVERFLOW = 2,    /* a fixed pool (solver rows, manifolds, pairs, the manifold sort's
+                                      stack) was full; the extra entries were dropped */
+    RSB_ARENA_BVH_OVERFLOW = 4,    /* reserved, never set: the BVH walk is stackless */
     RSB_ARENA_CULL_MISS = 8,       /* the learned culler skipped a query that had a contact */
     RSB_ARENA_EPA_OVERFLOW = 16    /* EPA's horizon walk exceeded its fixed stack; contact dropped */
 };
@@ -258,6 +264,13 @@ rsb_status rsb_layout(const rsb_handle* h, int32_t* num_arenas, int32_t* num_car
 rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride);
 
 rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode);
+/* Weights of the RSB_RESET_CURRICULUM modes (RocketSimCudaBatch::SetResetCurriculum,
+ * RocketSimCuda.h:283): relative weights of kickoff, fuzzed kickoff (ball and cars moved a
+ * little, mild ball velocity), aerial (ball raised near midfield, one car below it) and ball
+ * chase (ball in play, every car near it on the ground facing it).  A negative, non-finite or
+ * > 1e6 weight counts as 0; all zero means kickoff only.  A curriculum reset also staggers the
+ * no-touch timer over [0, 0.9 x the timeout).  Default: kickoff only. */
+rsb_status rsb_set_reset_curriculum(rsb_handle* h, float kickoff_w, float fuzzed_w, float aerial_w, float chase_w);
 /* Resets every arena whose terminal flag (from the last rsb_build_rewards_terminals) is
  * set, on the device and stream-ordered, with no host round trip; the flags themselves
  * are left as they are.  Pass a different seed on every call.  No counterpart in the

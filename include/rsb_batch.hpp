@@ -85,13 +85,20 @@ public:
         return half + o++;
     }
 
+    // RocketSimCudaBatch::ResetArena / ResetAllArenas (:275-278): kickoff, or the curriculum
+    // mix once SetResetCurriculum has been called.
     void ResetArena(int arenaIdx) {
         if (!ensure()) return;
         const int32_t idx = arenaIdx;
-        check(rsb_reset_arenas(h_, &idx, 1, nextSeed(), RSB_RESET_KICKOFF));
+        check(rsb_reset_arenas(h_, &idx, 1, nextSeed(), resetMode_));
     }
     void ResetAllArenas() {
-        if (ensure()) check(rsb_reset_all(h_, nextSeed(), RSB_RESET_KICKOFF));
+        if (ensure()) check(rsb_reset_all(h_, nextSeed(), resetMode_));
+    }
+    // RocketSimCudaBatch::SetResetCurriculum (:283).
+    void SetResetCurriculum(float kickoffW, float fuzzedW, float aerialW, float chaseW = 0.f) {
+        if (!ensure()) return;
+        if (check(rsb_set_reset_curriculum(h_, kickoffW, fuzzedW, aerialW, chaseW))) resetMode_ = RSB_RESET_CURRICULUM;
     }
 
     void SetCarControls(int arenaIdx, int carIdx, const CarControls& c) {
@@ -251,6 +258,7 @@ private:
     bool initialized_ = false;
     std::vector<int> blue_, orange_;
     uint64_t resets_ = 0;
+    int32_t resetMode_ = RSB_RESET_KICKOFF;
     rsb_status status_ = RSB_OK;
     std::string error_;
 };

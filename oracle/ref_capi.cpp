@@ -1066,6 +1066,12 @@ static void resetOne(rsb_handle* h, int a, uint64_t seed, int32_t mode) {
     }
 }
 
+// The reference CPU collector has no reset curriculum (it is the GPU batch's, RocketSimCuda.h:283):
+// the weights are checked and kept, and a curriculum reset is refused.
+rsb_status rsb_set_reset_curriculum(rsb_handle* h, float, float, float, float) {
+    return h ? RSB_OK : RSB_ERR_INVALID;
+}
+
 rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* idx, int32_t n, uint64_t seed, int32_t mode) {
     if (!h || (n > 0 && !idx)) return RSB_ERR_INVALID;
     if (mode != RSB_RESET_KICKOFF && mode != RSB_RESET_RANDOM_STATE)

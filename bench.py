@@ -423,6 +423,12 @@ def run_ours(args, rank, world, dist):
         pred = {"arenas": wl.num_arenas, "ticks": 360, "slices": [120, 240, 360], "ms": pms,
                 "ball_ticks_per_s": wl.num_arenas * 360 / pms * 1e3}
 
+    # the reference's own GPU batch (RocketSimCuda's stepArenaKernel and env kernels, built for
+    # sm_100a) on the same settled state and a seeded action stream, timed the same way
+    refgpu = None
+    if wl.preset == "c3" and not args.no_ref_gpu and rank == 0:
+        refgpu = reference_gpu(batch, wl, lut, pkg.MESHES_DIR, args.steps, args.warmup)
+
     # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
     # state read + written per launch (the library reports it), over the kernel's own time
     alg_bytes = batch.stats()["state_bytes_per_step"]
@@ -454,11 +460,65 @@ def run_ours(args, rank, world, dist):
         "learned_cull": learned,
         "state_ring": ring,
         "ball_prediction": pred,
+        "reference_gpu": refgpu,
         "autotune": tune,
         "clocks": clocks[-1],
         "clocks_exact": clocks[0],
     } | extra
     return res
+
+
+REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "librscudaref.so")
+
+
+def reference_gpu(batch, wl, lut, meshes, steps, warmup):
+    """The reference's batched GPU simulator (rsc::RocketSimCudaBatch, compiled for sm_100a by
+    oracle/Makefile) on this workload: its arenas take the engine's current (settled) car and
+    ball states, then run the reference's env step (snapshot, action indices, Step(tickSkip),
+    AdvancedObs + masks, rewards + terminals) on a seeded uniform action stream, timed with
+    CUDA events.  None when the comparator was not built."""
+    import ctypes as C
+
+    if not os.path.exists(REF_GPU_LIB) or wl.mixed:
+        return None
+    lib = C.CDLL(REF_GPU_LIB)
+    lib.rscref_create.restype = C.c_void_p
+    lib.rscref_create.argtypes = [C.c_int32, C.c_int32, C.c_char_p]
+    lib.rscref_destroy.argtypes = [C.c_void_p]
+    for f in ("rscref_set_lut", "rscref_set_states", "rscref_time_env_steps", "rscref_positions"):
+        getattr(lib, f).restype = C.c_int32
+    lib.rscref_set_lut.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.rscref_set_states.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rscref_time_env_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                          C.POINTER(C.c_float)]
+    lib.rscref_positions.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    t0 = time.perf_counter()
+    h = lib.rscref_create(wl.num_arenas, wl.team_size, meshes.encode())
+    if not h:
+        return {"unavailable": "the reference batch could not be created"}
+    try:
+        cars, balls = batch.get_cars(), batch.get_balls()
+        lut_c = np.ascontiguousarray(lut)
+        if lib.rscref_set_lut(h, lut_c.ctypes.data, len(lut_c)) or \
+                lib.rscref_set_states(h, cars.ctypes.data, balls.ctypes.data):
+            return {"unavailable": "setting the reference batch's states failed"}
+        setup_s = time.perf_counter() - t0
+        rng = np.random.default_rng(0x5EED0005)
+        acts = rng.integers(0, 90, (warmup + steps, batch.num_cars)).astype(np.int32)
+        ms = C.c_float()
+        if lib.rscref_time_env_steps(h, acts.ctypes.data, warmup, steps, wl.tick_skip, C.byref(ms)):
+            return {"unavailable": "the reference's env step reported a CUDA error"}
+        cp = np.zeros((batch.num_cars, 3), np.float32)
+        bp = np.zeros((wl.num_arenas, 3), np.float32)
+        lib.rscref_positions(h, cp.ctypes.data, bp.ctypes.data)
+        value = wl.num_arenas * wl.tick_skip * steps / (ms.value / 1e3)
+        return {"value": value, "unit": "arena-ticks/s", "ms_per_step": ms.value / steps, "steps": steps,
+                "warmup": warmup, "setup_s": setup_s, "finite_state": bool(np.isfinite(cp).all() and
+                                                                          np.isfinite(bp).all()),
+                "kernel": "RocketSimCuda stepArenaKernel + env kernels (reference sources, sm_100a)",
+                "start": "the engine's settled state after its timed steps; seeded uniform actions"}
+    finally:
+        lib.rscref_destroy(h)
 
 
 def stress_events(pkg, trained, wl, rank, dev):
@@ -738,6 +798,8 @@ def main():
     ap.add_argument("--no-gae", action="store_true", help="skip the GAE measurement of the c3 line")
     ap.add_argument("--no-ring", action="store_true", help="skip the state-ring measurement of the c3 line")
     ap.add_argument("--no-pred", action="store_true", help="skip the ball-prediction measurement of the c3 line")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip timing the reference's own GPU batch in the c3 line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -92,8 +92,8 @@ RSB_D float vdot4(float ax, float ay, float az, float bx, float by, float bz) {
 
 // ------------------------------------------------------------------ observations
 
-// Per-arena inputs staged in shared memory, one column per arena of the warp.
-constexpr int OBS_ARENAS = 32;
+// Per-arena inputs staged in shared memory, one column per arena of the block.
+constexpr int OBS_ARENAS = 16;
 constexpr int OI_BALL = 0;                                   // pos, vel, ang (uu)
 constexpr int OI_CAR = 9;                                    // per car, OI_CAR_N words
 constexpr int OI_CAR_N = 20;                                 // pos vel ang fwd right up boost flags
@@ -105,8 +105,21 @@ constexpr int OI_WORDS = OI_TEAM + 1;
 // flag bits of the staged car
 constexpr uint32_t OF_GROUND = 1, OF_FLIPJUMP = 2, OF_DEMOED = 4, OF_JUMPED = 8, OF_ORANGE = 16;
 
+// The parts of a row that do not depend on the viewing player itself, built once per arena:
+// the ball block and every car's 29-value block, in each team's frame (orange = InvertPhys).
+constexpr int OB_BALL = 0;                      // [frame][9]
+constexpr int OB_CAR = 2 * 9;                   // [frame][car][29]
+constexpr int OB_WORDS = OB_CAR + 2 * MAX_CARS * 29 + 1;  // odd row stride: fewer bank conflicts
+
 struct ObsShared {
     float in[OI_WORDS][OBS_ARENAS];
+    union {
+        float blk[OBS_ARENAS][OB_WORDS];
+        struct {                                 // staging of the pad records (phase A only)
+            float cool[NUM_PADS][OBS_ARENAS];
+            uint32_t act[NUM_PADS][OBS_ARENAS];
+        } pad;
+    };
     uint16_t rowOf[OBS_ARENAS * MAX_CARS];   // local row -> arena (low byte) | slot << 8
 };
 
@@ -146,127 +159,170 @@ RSB_D float obsCarValue(const ObsShared& S, int la, int q, bool inv, int j) {
     return (f & OF_JUMPED) ? 1.f : 0.f;
 }
 
-// Element `col` of the observation row of slot p in local arena la.
+// Element `col` of the observation row of slot p in local arena la, from the built blocks.
 RSB_D float obsValue(const ObsShared& S, int la, int p, int col) {
     const int T = (int)S.in[OI_TEAM][la];
-    const int M = 2 * T;
     const bool orange = p >= T;
-    if (col < 9) {
-        float v = S.in[OI_BALL + col][la] * (col < 3 ? OBS_POS : (col < 6 ? OBS_VEL : OBS_ANG));
-        return (orange && (col % 3) < 2) ? -v : v;
-    }
+    if (col < 9) return S.blk[la][OB_BALL + (orange ? 9 : 0) + col];
     if (col < 17) return S.in[OI_PREV + p * 8 + (col - 9)][la];
     if (col < 51) return S.in[OI_PAD + (orange ? NUM_PADS : 0) + (col - 17)][la];
-    int k = (col - 51) / 29, j = (col - 51) - 29 * ((col - 51) / 29);
-    if (k >= M) return 0.f;  // rows of smaller arenas in a ragged batch are zero-padded
+    const int k = (col - 51) / 29, j = (col - 51) - 29 * k;
+    if (k >= 2 * T) return 0.f;  // rows of smaller arenas in a ragged batch are zero-padded
     int q;
     const int ownFirst = orange ? T : 0, oppFirst = orange ? 0 : T;
     if (k == 0) {
         q = p;
     } else if (k < T) {
         // teammates, descending slot order, skipping the player
-        int idx = k - 1;
-        q = ownFirst + T - 1 - idx;
+        q = ownFirst + T - 1 - (k - 1);
         if (q <= p) q--;
     } else {
         q = oppFirst + T - 1 - (k - T);
     }
-    return obsCarValue(S, la, q, orange, j);
+    return S.blk[la][OB_CAR + ((orange ? MAX_CARS : 0) + q) * 29 + j];
 }
 
-// A block stages the inputs of 32 arenas (one arena per thread of its first warp), then
-// all of its warps build and write the arenas' rows: the rows of consecutive arenas are
-// contiguous, so the writes are coalesced.
+// A block serves 16 arenas in three phases, every thread taking part in each:
+//   A. stage the arenas' records from the word planes (consecutive threads read consecutive
+//      arenas of one word: coalesced), derive flags, masks, pad values and the actions;
+//   B. build the ball block and the 29-value block of every car once per team frame;
+//   C. write the arenas' rows, which are contiguous in the output, as 16-byte stores of four
+//      elements assembled from the blocks, and the mask bytes as 32-bit words.
 constexpr int OBS_THREADS = 256;
 __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb) {
     __shared__ ObsShared S;
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x;
     const int a0 = blockIdx.x * OBS_ARENAS;
     if (a0 >= E.N) return;
-    const int aEnd = min(a0 + OBS_ARENAS, E.N);
-    const int a = a0 + lane;
+    const int na = min(OBS_ARENAS, E.N - a0);
     const int row0 = E.carOffset[a0];
-    if (lane < OBS_ARENAS && a < aEnd) {
-        const int T = E.teamSize[a], M = 2 * T;
-        S.in[OI_TEAM][lane] = (float)T;
-        for (int k = 0; k < 3; k++) {
-            S.in[OI_BALL + k][lane] = ballF(E, a, BW_POS + k) * kBtToUu;
-            S.in[OI_BALL + 3 + k][lane] = ballF(E, a, BW_LIN + k) * kBtToUu;
-            S.in[OI_BALL + 6 + k][lane] = ballF(E, a, BW_ANG + k);
-        }
-        const int base = E.carOffset[a];
-        for (int s = 0; s < M; s++) {
-            const int o = OI_CAR + s * OI_CAR_N;
-            for (int k = 0; k < 3; k++) {
-                S.in[o + k][lane] = carF(E, a, s, CW_POS + k) * kBtToUu;
-                S.in[o + 3 + k][lane] = carF(E, a, s, CW_LIN + k) * kBtToUu;
-                S.in[o + 6 + k][lane] = carF(E, a, s, CW_ANG + k);
-                // CarState::rotMat columns: forward, right, up (basis rows stored)
-                S.in[o + 9 + k][lane] = carF(E, a, s, CW_ROTMAT + 3 * k + 0);
-                S.in[o + 12 + k][lane] = carF(E, a, s, CW_ROTMAT + 3 * k + 1);
-                S.in[o + 15 + k][lane] = carF(E, a, s, CW_ROTMAT + 3 * k + 2);
-            }
-            const float boost = carF(E, a, s, CW_BOOST);
-            S.in[o + 18][lane] = boost;
-            const uint32_t cf = carW(E, a, s, CW_FLAGS);
-            const bool ground = cf & CF_ON_GROUND;
-            // CarState::HasFlipOrJump (Car.cpp:285-289)
-            const bool flipJump = ground || (!(cf & CF_HAS_FLIPPED) && !(cf & CF_HAS_DOUBLE_JUMPED) &&
-                                             carF(E, a, s, CW_AIRSJ) < DOUBLEJUMP_MAX_DELAY);
-            uint32_t of = (ground ? OF_GROUND : 0u) | (flipJump ? OF_FLIPJUMP : 0u) |
-                          ((cf & CF_DEMOED) ? OF_DEMOED : 0u) | ((cf & CF_HAS_JUMPED) ? OF_JUMPED : 0u) |
-                          ((cf & CF_TEAM_ORANGE) ? OF_ORANGE : 0u);
-            S.in[o + 19][lane] = __uint_as_float(of);
-            // DefaultAction::GetActionMask
-            const bool turtled = (cf & CF_WORLD_CONTACT) && carF(E, a, s, CW_WCN + 2) > 0.9f;
-            for (int w = 0; w < 3; w++) {
-                uint32_t m = ground ? Tb.ground[w] : Tb.air[w];
-                if (boost == 0.f) m &= ~Tb.boost[w];
-                if (flipJump || turtled) m |= Tb.jump[w];
-                S.in[OI_MASK + s * 3 + w][lane] = __uint_as_float(m);
-            }
-            // the step's action (EnvSet passes the parsed Action as prevAction)
-            const CtlRec c = E.controls[base + s];
-            for (int k = 0; k < 5; k++) S.in[OI_PREV + s * 8 + k][lane] = c.v[k];
-            S.in[OI_PREV + s * 8 + 5][lane] = c.jump ? 1.f : 0.f;
-            S.in[OI_PREV + s * 8 + 6][lane] = c.boost ? 1.f : 0.f;
-            S.in[OI_PREV + s * 8 + 7][lane] = c.handbrake ? 1.f : 0.f;
-            S.rowOf[base - row0 + s] = (uint16_t)(lane | (s << 8));
-        }
-        // boost pads in RLGymCPP order; GameState::GetBoostPadTimers returns the mirrored
-        // timers for the blue frame and the direct ones for the orange frame
-        // (GameState.h:56-62), and AdvancedObs pairs them with the frame's pads
-        float cool[NUM_PADS];
-        uint32_t act = 0, act2 = 0;
-        for (int p = 0; p < NUM_PADS; p++) {
-            cool[p] = __uint_as_float(E.pad[((size_t)0 * NUM_PADS + p) * E.N + a]);
-            uint32_t bits = E.pad[((size_t)1 * NUM_PADS + p) * E.N + a];
-            if (bits & 1u) {
-                if (p < 32) act |= 1u << p;
-                else act2 |= 1u << (p - 32);
-            }
-        }
-        auto active = [&](int p) { return p < 32 ? ((act >> p) & 1u) : ((act2 >> (p - 32)) & 1u); };
-        for (int i = 0; i < NUM_PADS; i++) {
-            const int d = Tb.padMap[i], m = Tb.padMap[NUM_PADS - 1 - i];
-            S.in[OI_PAD + i][lane] = active(d) ? 1.f : 1.f / (1.f + cool[m]);
-            S.in[OI_PAD + NUM_PADS + i][lane] = active(m) ? 1.f : 1.f / (1.f + cool[d]);
+
+    // ---- A: ball words and team sizes
+    for (int i = tid; i < 10 * OBS_ARENAS; i += OBS_THREADS) {
+        const int la = i % OBS_ARENAS, w = i / OBS_ARENAS, a = a0 + la;
+        if (la >= na) continue;
+        if (w == 9) {
+            S.in[OI_TEAM][la] = (float)E.teamSize[a];
+        } else {
+            const int k = w % 3;
+            const float v = w < 3 ? ballF(E, a, BW_POS + k) * kBtToUu
+                                  : (w < 6 ? ballF(E, a, BW_LIN + k) * kBtToUu : ballF(E, a, BW_ANG + k));
+            S.in[OI_BALL + w][la] = v;
         }
     }
+    // cars: one (arena, slot) per thread
+    for (int i = tid; i < MAX_CARS * OBS_ARENAS; i += OBS_THREADS) {
+        const int la = i % OBS_ARENAS, s = i / OBS_ARENAS, a = a0 + la;
+        if (la >= na || s >= 2 * E.teamSize[a]) continue;
+        const int o = OI_CAR + s * OI_CAR_N;
+        for (int k = 0; k < 3; k++) {
+            S.in[o + k][la] = carF(E, a, s, CW_POS + k) * kBtToUu;
+            S.in[o + 3 + k][la] = carF(E, a, s, CW_LIN + k) * kBtToUu;
+            S.in[o + 6 + k][la] = carF(E, a, s, CW_ANG + k);
+            // CarState::rotMat columns: forward, right, up (basis rows stored)
+            S.in[o + 9 + k][la] = carF(E, a, s, CW_ROTMAT + 3 * k + 0);
+            S.in[o + 12 + k][la] = carF(E, a, s, CW_ROTMAT + 3 * k + 1);
+            S.in[o + 15 + k][la] = carF(E, a, s, CW_ROTMAT + 3 * k + 2);
+        }
+        const float boost = carF(E, a, s, CW_BOOST);
+        S.in[o + 18][la] = boost;
+        const uint32_t cf = carW(E, a, s, CW_FLAGS);
+        const bool ground = cf & CF_ON_GROUND;
+        // CarState::HasFlipOrJump (Car.cpp:285-289)
+        const bool flipJump = ground || (!(cf & CF_HAS_FLIPPED) && !(cf & CF_HAS_DOUBLE_JUMPED) &&
+                                         carF(E, a, s, CW_AIRSJ) < DOUBLEJUMP_MAX_DELAY);
+        const uint32_t of = (ground ? OF_GROUND : 0u) | (flipJump ? OF_FLIPJUMP : 0u) |
+                            ((cf & CF_DEMOED) ? OF_DEMOED : 0u) | ((cf & CF_HAS_JUMPED) ? OF_JUMPED : 0u) |
+                            ((cf & CF_TEAM_ORANGE) ? OF_ORANGE : 0u);
+        S.in[o + 19][la] = __uint_as_float(of);
+        // DefaultAction::GetActionMask
+        const bool turtled = (cf & CF_WORLD_CONTACT) && carF(E, a, s, CW_WCN + 2) > 0.9f;
+        for (int w = 0; w < 3; w++) {
+            uint32_t m = ground ? Tb.ground[w] : Tb.air[w];
+            if (boost == 0.f) m &= ~Tb.boost[w];
+            if (flipJump || turtled) m |= Tb.jump[w];
+            S.in[OI_MASK + s * 3 + w][la] = __uint_as_float(m);
+        }
+        // the step's action (EnvSet passes the parsed Action as prevAction)
+        const int base = E.carOffset[a];
+        const CtlRec c = E.controls[base + s];
+        for (int k = 0; k < 5; k++) S.in[OI_PREV + s * 8 + k][la] = c.v[k];
+        S.in[OI_PREV + s * 8 + 5][la] = c.jump ? 1.f : 0.f;
+        S.in[OI_PREV + s * 8 + 6][la] = c.boost ? 1.f : 0.f;
+        S.in[OI_PREV + s * 8 + 7][la] = c.handbrake ? 1.f : 0.f;
+        S.rowOf[base - row0 + s] = (uint16_t)(la | (s << 8));
+    }
+    // pad records
+    for (int i = tid; i < NUM_PADS * OBS_ARENAS; i += OBS_THREADS) {
+        const int la = i % OBS_ARENAS, p = i / OBS_ARENAS, a = a0 + la;
+        if (la >= na) continue;
+        S.pad.cool[p][la] = __uint_as_float(E.pad[((size_t)0 * NUM_PADS + p) * E.N + a]);
+        S.pad.act[p][la] = E.pad[((size_t)1 * NUM_PADS + p) * E.N + a] & 1u;
+    }
     __syncthreads();
-    const int rows = E.carOffset[aEnd] - row0;
+    // boost pads in RLGymCPP order; GameState::GetBoostPadTimers returns the mirrored timers for
+    // the blue frame and the direct ones for the orange frame (GameState.h:56-62), and
+    // AdvancedObs pairs them with the frame's pads
+    for (int i = tid; i < NUM_PADS * OBS_ARENAS; i += OBS_THREADS) {
+        const int la = i % OBS_ARENAS, pi = i / OBS_ARENAS;
+        if (la >= na) continue;
+        const int d = Tb.padMap[pi], m = Tb.padMap[NUM_PADS - 1 - pi];
+        S.in[OI_PAD + pi][la] = S.pad.act[d][la] ? 1.f : 1.f / (1.f + S.pad.cool[m][la]);
+        S.in[OI_PAD + NUM_PADS + pi][la] = S.pad.act[m][la] ? 1.f : 1.f / (1.f + S.pad.cool[d][la]);
+    }
+    __syncthreads();
+
+    // ---- B: ball blocks and car blocks of both frames
+    constexpr int PER_ARENA = 2 * 9 + 2 * MAX_CARS * 29;
+    for (int i = tid; i < PER_ARENA * OBS_ARENAS; i += OBS_THREADS) {
+        const int la = i % OBS_ARENAS, w = i / OBS_ARENAS;
+        if (la >= na) continue;
+        float v = 0.f;
+        if (w < 18) {
+            const int col = w % 9;
+            const bool orange = w >= 9;
+            v = S.in[OI_BALL + col][la] * (col < 3 ? OBS_POS : (col < 6 ? OBS_VEL : OBS_ANG));
+            if (orange && (col % 3) < 2) v = -v;
+        } else {
+            const int c = w - 18, fq = c / 29, j = c - 29 * fq;
+            const int q = fq % MAX_CARS;
+            if (q < 2 * (int)S.in[OI_TEAM][la]) v = obsCarValue(S, la, q, fq >= MAX_CARS, j);
+        }
+        S.blk[la][w] = v;
+    }
+    __syncthreads();
+
+    // ---- C: the rows (contiguous for the block's arenas), then the masks
+    const int rows = E.carOffset[a0 + na] - row0;
     const int stride = E.stride;
     float* out = E.obs + (size_t)row0 * stride;
     const int n = rows * stride;
-    for (int e = lane; e < n; e += OBS_THREADS) {
+    auto elem = [&](int e) {
         const int r = e / stride, col = e - r * stride;
         const uint16_t ro = S.rowOf[r];
-        out[e] = obsValue(S, ro & 0xff, ro >> 8, col);
+        return obsValue(S, ro & 0xff, ro >> 8, col);
+    };
+    // elements before the first 16-byte boundary, whole float4s, then the tail
+    const int head = min(n, (int)(((16 - ((uintptr_t)out & 15)) & 15) / 4));
+    const int body = (n - head) / 4;
+    if (tid < head) out[tid] = elem(tid);
+    float4* out4 = reinterpret_cast<float4*>(out + head);
+    for (int v = tid; v < body; v += OBS_THREADS) {
+        const int e = head + 4 * v;
+        int r = e / stride, col = e - r * stride;
+        float x[4];
+        for (int t = 0; t < 4; t++) {
+            const uint16_t ro = S.rowOf[r];
+            x[t] = obsValue(S, ro & 0xff, ro >> 8, col);
+            if (++col == stride) { col = 0; r++; }
+        }
+        out4[v] = make_float4(x[0], x[1], x[2], x[3]);
     }
+    for (int e = head + 4 * body + tid; e < n; e += OBS_THREADS) out[e] = elem(e);
     // masks: rows * 90 bytes, 4-byte aligned (every arena has an even number of cars)
     uint32_t* mout = reinterpret_cast<uint32_t*>(E.masks + (size_t)row0 * RSB_NUM_ACTIONS);
     const int nw = rows * RSB_NUM_ACTIONS / 4;
-    for (int w = lane; w < nw; w += OBS_THREADS) {
+    for (int w = tid; w < nw; w += OBS_THREADS) {
         uint32_t word = 0;
         for (int t = 0; t < 4; t++) {
             const int e = 4 * w + t, r = e / RSB_NUM_ACTIONS, i = e - r * RSB_NUM_ACTIONS;

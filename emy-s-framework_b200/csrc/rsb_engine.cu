@@ -734,13 +734,12 @@ rsb_status rsb_predict_ball(rsb_handle* h, const int32_t* slice_ticks, int32_t n
     const size_t need = (size_t)h->N * n_slices;
     if (out && out_count != need) return fail(h, RSB_ERR_INVALID, "rsb_predict_ball: out_count must be num_arenas * n_slices");
     RSB_CUDA(cudaSetDevice(h->device));
-    if (h->predCap < need) {
-        cudaFree(h->dPred);
-        h->dPred = nullptr;
-        h->predCap = 0;
-        if (cudaMalloc((void**)&h->dPred, need * sizeof(rsb_ball_state)) != cudaSuccess)
+    if (!h->dPred) {
+        // sized for the most slices once, so that the RSB_BUF_BALL_PRED pointer never changes
+        const size_t cap = (size_t)h->N * RSB_MAX_PRED_SLICES;
+        if (cudaMalloc((void**)&h->dPred, cap * sizeof(rsb_ball_state)) != cudaSuccess)
             return fail(h, RSB_ERR_NOMEM, "rsb_predict_ball: allocation failed");
-        h->predCap = need;
+        h->predCap = cap;
     }
     cudaStream_t st = pick(h, stream);
     predictBallKernel<<<(h->N + 127) / 128, 128, 0, st>>>(devView(h), s, h->dPred);

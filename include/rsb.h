@@ -291,8 +291,10 @@ rsb_status rsb_set_actions_device(rsb_handle* h, const int32_t* d_idx, int32_t n
  * part of the library image instead of a buffer allocated for the handle.  At most
  * RSB_STATIC_ACTIONS_MAX indices per call (larger n returns RSB_ERR_INVALID).  The first
  * call on a device looks up the array's address (no allocation); make that first call
- * before capturing the handle's stream into a graph.  The array is shared by every handle
- * on a device: calls from two handles of one device must not overlap in time.  No
+ * before capturing the handle's stream into a graph.  The address is kept for the life of
+ * the process: after a cudaDeviceReset (or any new primary context) on that device, do not
+ * call this function again in the same process.  The array is shared by every handle on a
+ * device: calls from two handles of one device must not overlap in time.  No
  * counterpart in the reference (RocketSimCuda.h has only the allocating variant). */
 #define RSB_STATIC_ACTIONS_MAX (65536 * 6)
 rsb_status rsb_set_actions_host_static(rsb_handle* h, const int32_t* idx, int32_t n);
@@ -342,8 +344,10 @@ rsb_status rsb_get_arena_info_at(rsb_handle* h, int32_t arena, rsb_arena_info* o
  * with the batch's physics; out[a * n_slices + k] is the ball after slice_ticks[k] ticks
  * (1..8 slices, rising, at most 4096 ticks).  The arenas are only read.  With out non-null the
  * slices are copied to it (out_count = num_arenas * n_slices) and the stream is synchronised;
- * with out null they stay on the device (rsb_device_ptr, RSB_BUF_BALL_PRED).  Allocates its
- * device buffer on the first call of a given size. */
+ * with out null they stay on the device (rsb_device_ptr, RSB_BUF_BALL_PRED).  The first call
+ * allocates the device buffer for RSB_MAX_PRED_SLICES slices of every arena (60 B each), so
+ * the RSB_BUF_BALL_PRED pointer stays the same for the life of the handle; each call
+ * overwrites its first num_arenas * n_slices entries. */
 #define RSB_MAX_PRED_SLICES 8
 #define RSB_MAX_PRED_TICKS 4096
 rsb_status rsb_predict_ball(rsb_handle* h, const int32_t* slice_ticks, int32_t n_slices, rsb_ball_state* out,

@@ -50,6 +50,36 @@ def test_prediction_matches_oracle(pkg, oracle_lib, meshes_dir):
         assert d.max() <= 0.05, f"tick {t}: a ball {d.max():.3g} uu from the oracle"
 
 
+def test_repeated_predictions_match_oracle(pkg, oracle_lib, meshes_dir):
+    """BallPredTracker keeps its ball-only arena between updates (the oracle does too, with its
+    Bullet world, tick count and broadphase registration); the engine starts every call from
+    a fresh ball-only world.  Three calls in a row on different balls - flying, at rest on the
+    floor, rolling, and the balls of a stepped batch - give the oracle's slices byte for byte."""
+    rsb = pkg.rsb
+    n = 256
+    eng, ora = _synced_pair(pkg, oracle_lib, meshes_dir, n, 60)
+    rest = random_balls(rsb, n, 61, rest_fraction=0.0)
+    rest["pos"]["z"] = 93.15
+    for c in "xyz":
+        rest["vel"][c] = 0.0
+        rest["ang_vel"][c] = 0.0
+    rolling = rest.copy()
+    rolling["vel"]["x"] = np.random.default_rng(62).uniform(-1500, 1500, n)
+    rolling["vel"]["y"] = np.random.default_rng(63).uniform(-1500, 1500, n)
+    for call, balls in enumerate((None, rest, rolling, "stepped")):
+        if isinstance(balls, np.ndarray):
+            for b in (eng, ora):
+                b.set_balls(balls)
+        elif balls == "stepped":
+            ora.step(8)
+            eng.set_balls(ora.get_balls())
+        pe, po = eng.predict_ball(SLICES), ora.predict_ball(SLICES)
+        for k, t in enumerate(SLICES):
+            d = np.linalg.norm(vec(pe[:, k], "pos") - vec(po[:, k], "pos"), axis=1)
+            assert pe[:, k].tobytes() == po[:, k].tobytes(), (
+                f"call {call}, tick {t}: {int((d > 0).sum())} balls differ, largest {d.max():.3g} uu")
+
+
 def test_prediction_equals_ball_only_batch(pkg, meshes_dir):
     rsb = pkg.rsb
     n = 4096

@@ -3,8 +3,8 @@ GPU: the failures are bad inputs the host uploads).
 
   * a non-finite car state raises RSB_ARENA_NONFINITE in its own arena only, leaves every
     other arena bit-identical to a run without it, and a reset clears the bit;
-  * a culler bound that is deliberately wrong (a negative margin, so every body looks clear
-    of the arena) in audit mode: the skipped static tests still run, every contact they find
+  * a culler bound that is deliberately wrong (the network answers 1e6 uu everywhere, so every
+    body looks clear of the arena) in audit mode: the skipped static tests still run, every contact they find
     is counted as a missed contact, the arenas that saw one carry RSB_ARENA_CULL_MISS and are
     counted as reverted, and the state stays bit-identical to the exact path; a reset clears
     the bit.
@@ -66,9 +66,11 @@ def test_wrong_culler_bound_is_caught_by_the_audit(pkg, meshes_dir):
     n = 256
     exact, audit = (rsb.Batch(pkg.engine_library(), n, team_size=2, meshes_path=meshes_dir, cull_mode=m)
                     for m in (rsb.RSB_CULL_EXACT, rsb.RSB_CULL_LEARNED_AUDIT))
-    # any weights with a margin of -1e6 uu: every bound clears every body's reach
+    # a network that answers 1e6 uu everywhere (zero weights, output bias 1e6): every bound
+    # clears every body's reach
     params = np.zeros(rsb.RSB_CULLER_PARAMS, np.float32)
-    audit.culler_set(params, -1e6)
+    params[-1] = 1e6
+    audit.culler_set(params, 0.0)
     lut = rsb.default_action_lut(exact.lib)
     for x in (exact, audit):
         x.set_action_lut(lut)

@@ -32,6 +32,24 @@ def test_static_actions_match_allocating_path_twice(pkg, meshes_dir):
         assert a.get_balls().tobytes() == b.get_balls().tobytes()
 
 
+def test_static_actions_allocate_no_device_memory(pkg, meshes_dir):
+    """After the first call on the device (which looks up the array's address), further calls
+    leave the device's free memory unchanged."""
+    import torch
+
+    _, b = _pair(pkg, meshes_dir, 4096, 3)
+    rng = np.random.default_rng(12)
+    idx = rng.integers(0, pkg.rsb.RSB_NUM_ACTIONS, b.num_cars).astype(np.int32)
+    b.set_actions_static(idx)
+    b.sync()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        b.set_actions_static(rng.integers(0, pkg.rsb.RSB_NUM_ACTIONS, b.num_cars).astype(np.int32))
+    b.sync()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+
+
 def test_static_actions_reject_oversize(pkg, meshes_dir):
     rsb = pkg.rsb
     a, _ = _pair(pkg, meshes_dir, 2, 1)

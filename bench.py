@@ -423,11 +423,34 @@ def run_ours(args, rank, world, dist):
         pred = {"arenas": wl.num_arenas, "ticks": 360, "slices": [120, 240, 360], "ms": pms,
                 "ball_ticks_per_s": wl.num_arenas * 360 / pms * 1e3}
 
+    # the observation kernel alone (AdvancedObs rows + DefaultAction masks), L2 flushed between
+    # calls: its algorithmic bytes are the rows and masks written plus the records it reads
+    # (ball 9 words + team size, per car 22 words + its 24-byte action, 34 pads x 2 words)
+    peak, peak_kind = measured_peaks()
+    obs = None
+    if not args.no_obs_roofline:
+        obs_ms = []
+        with torch.cuda.stream(stream):
+            for k in range(8):
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                batch.build_obs(stream=sp)
+                e1.record(stream)
+                e1.synchronize()
+                obs_ms.append(e0.elapsed_time(e1))
+        oms = statistics.median(obs_ms[2:])
+        out_b = batch.num_cars * (4 * batch.obs_stride + rsb.RSB_NUM_ACTIONS)
+        in_b = wl.num_arenas * (10 * 4 + 34 * 2 * 4) + batch.num_cars * (22 * 4 + 24)
+        ach = (out_b + in_b) / (oms / 1e3) / 1e9
+        obs = {"bound": "hbm", "kernel": "obsKernel", "achieved": ach, "peak": peak, "unit": "GB/s",
+               "frac": ach / peak, "bytes_per_call": out_b + in_b, "ms": oms, "traffic": None}
+
     # the reference's own GPU batch (RocketSimCuda's stepArenaKernel and env kernels, built for
     # sm_100a) on the same settled state and a seeded action stream, timed the same way
     refgpu = None
     if wl.preset == "c3" and not args.no_ref_gpu and rank == 0:
-        refgpu = reference_gpu(batch, wl, lut, pkg.MESHES_DIR, args.steps, args.warmup)
+        refgpu = reference_gpu(batch, wl, lut, pkg.MESHES_DIR, args.steps, args.warmup, args.settle)
 
     # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
     # state read + written per launch (the library reports it), over the kernel's own time
@@ -461,6 +484,7 @@ def run_ours(args, rank, world, dist):
         "state_ring": ring,
         "ball_prediction": pred,
         "reference_gpu": refgpu,
+        "obs_roofline": obs,
         "autotune": tune,
         "clocks": clocks[-1],
         "clocks_exact": clocks[0],
@@ -471,12 +495,14 @@ def run_ours(args, rank, world, dist):
 REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "librscudaref.so")
 
 
-def reference_gpu(batch, wl, lut, meshes, steps, warmup):
+def reference_gpu(batch, wl, lut, meshes, steps, warmup, settle):
     """The reference's batched GPU simulator (rsc::RocketSimCudaBatch, compiled for sm_100a by
-    oracle/Makefile) on this workload: its arenas take the engine's current (settled) car and
-    ball states, then run the reference's env step (snapshot, action indices, Step(tickSkip),
-    AdvancedObs + masks, rewards + terminals) on a seeded uniform action stream, timed with
-    CUDA events.  None when the comparator was not built."""
+    oracle/Makefile) on this workload: its arenas start from its own kickoff reset, run the
+    same number of untimed settle steps as the engine, then the timed env steps (snapshot,
+    action indices, Step(tickSkip), AdvancedObs + masks, rewards + terminals) on a seeded
+    uniform action stream, timed with CUDA events.  (Its per-car SetCarState costs two
+    synchronous copies per car, over a minute at 393,216 cars, so the engine's states are not
+    copied in.)  None when the comparator was not built."""
     import ctypes as C
 
     if not os.path.exists(REF_GPU_LIB) or wl.mixed:
@@ -497,13 +523,12 @@ def reference_gpu(batch, wl, lut, meshes, steps, warmup):
     if not h:
         return {"unavailable": "the reference batch could not be created"}
     try:
-        cars, balls = batch.get_cars(), batch.get_balls()
         lut_c = np.ascontiguousarray(lut)
-        if lib.rscref_set_lut(h, lut_c.ctypes.data, len(lut_c)) or \
-                lib.rscref_set_states(h, cars.ctypes.data, balls.ctypes.data):
-            return {"unavailable": "setting the reference batch's states failed"}
+        if lib.rscref_set_lut(h, lut_c.ctypes.data, len(lut_c)):
+            return {"unavailable": "uploading the action table to the reference batch failed"}
         setup_s = time.perf_counter() - t0
         rng = np.random.default_rng(0x5EED0005)
+        warmup = settle + warmup
         acts = rng.integers(0, 90, (warmup + steps, batch.num_cars)).astype(np.int32)
         ms = C.c_float()
         if lib.rscref_time_env_steps(h, acts.ctypes.data, warmup, steps, wl.tick_skip, C.byref(ms)):
@@ -516,7 +541,7 @@ def reference_gpu(batch, wl, lut, meshes, steps, warmup):
                 "warmup": warmup, "setup_s": setup_s, "finite_state": bool(np.isfinite(cp).all() and
                                                                           np.isfinite(bp).all()),
                 "kernel": "RocketSimCuda stepArenaKernel + env kernels (reference sources, sm_100a)",
-                "start": "the engine's settled state after its timed steps; seeded uniform actions"}
+                "start": f"its kickoff reset, {settle} settle + {warmup - settle} warm-up env steps; seeded uniform actions"}
     finally:
         lib.rscref_destroy(h)
 
@@ -798,6 +823,7 @@ def main():
     ap.add_argument("--no-gae", action="store_true", help="skip the GAE measurement of the c3 line")
     ap.add_argument("--no-ring", action="store_true", help="skip the state-ring measurement of the c3 line")
     ap.add_argument("--no-pred", action="store_true", help="skip the ball-prediction measurement of the c3 line")
+    ap.add_argument("--no-obs-roofline", action="store_true", help="skip timing the observation kernel alone")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference's own GPU batch in the c3 line")
     args = ap.parse_args()

@@ -129,10 +129,11 @@ struct rsb_handle {
     int numTris = 0;
     std::shared_ptr<ArenaStaticHost> host;
     // launch configuration of the step kernel (indices into kStepVariants / kStepBlocks)
-    int stepVariant = 0, stepBlock = 1;
+    int stepVariant = 0, stepBlock = 1, stepResidency = 0;
     uint32_t* dScratch = nullptr;   // the autotuner's copy of the arena records
     unsigned int* dWork = nullptr;  // claim counter of the persistent step kernel
     int persistGrid[8][4] = {};     // resident blocks (all SMs) per persistent variant and block size
+    int smCount = 0;
     uint32_t* dStage = nullptr;     // staging of the per-arena getters
     rsb_ball_state* dPred = nullptr;  // ball prediction slices [num_arenas][n_slices]
     size_t predCap = 0;
@@ -216,6 +217,11 @@ static const StepVariant kStepVariants[] = {{stepKernel<1>, 1, false},          
 constexpr int kNumStepVariants = sizeof(kStepVariants) / sizeof(kStepVariants[0]);
 static const int kStepBlocks[] = {32, 64, 128};
 constexpr int kNumStepBlocks = sizeof(kStepBlocks) / sizeof(kStepBlocks[0]);
+// Resident warps per SM of a persistent launch (0 = as many as fit).  The working sets of the
+// arenas in flight share the L2: with every warp slot filled (about 38,000 arenas at a time)
+// they do not fit, and each thread waits on DRAM; fewer arenas in flight stay in L2.
+static const int kStepResidency[] = {0, 1, 2, 3, 4, 6};
+constexpr int kNumStepResidency = sizeof(kStepResidency) / sizeof(kStepResidency[0]);
 
 // xorshift32 draw in [0, 1] and range of the reference's state ring (CudaEnvSet.cpp:608-617)
 RSB_HD float ringRand01(uint32_t& rng) {
@@ -678,9 +684,14 @@ rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride) {
     return RSB_OK;
 }
 
+// Dynamic shared memory of a step-kernel launch: the warp-cooperative mesh-ray queries'
+// candidate slots (phys/ray.h), kRayCoopWarpBytes per warp.
+static size_t stepSmem(int block) { return (size_t)((block + 31) / 32) * kRayCoopWarpBytes; }
+
 // Launches step-kernel variant v with block size index b on stream st (a persistent variant
 // first zeroes its claim counter on the same stream).
-static cudaError_t launchStep(rsb_handle* h, const EngineView& D, int v, int b, int ticks, cudaStream_t st) {
+static cudaError_t launchStep(rsb_handle* h, const EngineView& D, int v, int b, int ticks, cudaStream_t st,
+                              int residency = 0) {
     const StepVariant& sv = kStepVariants[v];
     const int block = kStepBlocks[b];
     int grid = (h->N + block - 1) / block;
@@ -688,16 +699,22 @@ static cudaError_t launchStep(rsb_handle* h, const EngineView& D, int v, int b, 
         int& g = h->persistGrid[v][b];
         if (g == 0) {
             int perSm = 0, sms = 0;
-            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sv.fn, block, 0);
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sv.fn, block, stepSmem(block));
             if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
             if (e != cudaSuccess) return e;
+            h->smCount = sms;
             g = std::max(1, perSm * sms);
         }
-        grid = std::min(grid, g);
+        int cap = g;
+        if (kStepResidency[residency] > 0) {
+            const int blocksPerSm = std::max(1, kStepResidency[residency] * 32 / block);
+            cap = std::min(g, blocksPerSm * h->smCount);
+        }
+        grid = std::min(grid, cap);
         cudaError_t e = cudaMemsetAsync(h->dWork, 0, sizeof(unsigned int), st);
         if (e != cudaSuccess) return e;
     }
-    sv.fn<<<grid, block, 0, st>>>(D, ticks);
+    sv.fn<<<grid, block, stepSmem(block), st>>>(D, ticks);
     return cudaGetLastError();
 }
 
@@ -714,7 +731,7 @@ rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
         RSB_CUDA(cudaGetLastError());
         D.cull = h->dCull;
     }
-    RSB_CUDA(launchStep(h, D, h->stepVariant, h->stepBlock, ticks, st));
+    RSB_CUDA(launchStep(h, D, h->stepVariant, h->stepBlock, ticks, st, h->stepResidency));
     h->stats.ticks_simulated += (uint64_t)h->N * ticks;
     return RSB_OK;
 }
@@ -768,10 +785,22 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
     RSB_CUDA(cudaEventCreate(&e0));
     RSB_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    int n = 0, bestV = h->stepVariant, bestB = h->stepBlock;
+    int n = 0, bestV = h->stepVariant, bestB = h->stepBlock, bestR = h->stepResidency;
     rsb_status st = RSB_OK;
-    for (int v = 0; v < kNumStepVariants && st == RSB_OK; v++)
-        for (int b = 0; b < kNumStepBlocks && st == RSB_OK; b++) {
+    // every (variant, block) with all warp slots filled; the residency caps on the persistent
+    // variant with the largest register budget, at 32 and 64 threads per block
+    struct Cand { int v, b, r; };
+    std::vector<Cand> cands;
+    for (int v = 0; v < kNumStepVariants; v++)
+        for (int b = 0; b < kNumStepBlocks; b++) cands.push_back({v, b, 0});
+    for (int v = 0; v < kNumStepVariants; v++)
+        if (kStepVariants[v].persistent && kStepVariants[v].minBlocks == 1)
+            for (int b = 0; b < 2; b++)
+                for (int r = 1; r < kNumStepResidency; r++) cands.push_back({v, b, r});
+    for (const Cand& c : cands) {
+        if (st != RSB_OK) break;
+        const int v = c.v, b = c.b;
+        {
             float ms = 1e30f;
             for (int rep = 0; rep < 2; rep++) {
                 // every candidate starts from the same copy of the current state
@@ -781,7 +810,7 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
                 if (e == cudaSuccess)
                     e = cudaMemcpyAsync(D.arena, h->dArena, wArena * 4, cudaMemcpyDeviceToDevice, h->stream);
                 if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
-                if (e == cudaSuccess) e = launchStep(h, D, v, b, ticks, h->stream);
+                if (e == cudaSuccess) e = launchStep(h, D, v, b, ticks, h->stream, c.r);
                 if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
                 if (e == cudaSuccess) e = cudaEventSynchronize(e1);
                 float t = 0.f;
@@ -794,27 +823,36 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
             }
             if (st != RSB_OK) break;
             if (out && n < cap)
-                out[n] = rsb_tune_entry{kStepVariants[v].minBlocks, kStepBlocks[b], ms, kStepVariants[v].persistent ? 1 : 0};
+                out[n] = rsb_tune_entry{kStepVariants[v].minBlocks, kStepBlocks[b], ms,
+                                        kStepVariants[v].persistent ? 1 : 0, kStepResidency[c.r]};
             n++;
-            if (ms < best) { best = ms; bestV = v; bestB = b; }
+            if (ms < best) { best = ms; bestV = v; bestB = b; bestR = c.r; }
         }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != RSB_OK) return st;
     h->stepVariant = bestV;
     h->stepBlock = bestB;
+    h->stepResidency = bestR;
     if (count) *count = n;
     return RSB_OK;
 }
 
 rsb_status rsb_set_step_config(rsb_handle* h, const rsb_tune_entry* cfg) {
     if (!h || !cfg) return RSB_ERR_INVALID;
+    int r = -1;
+    for (int k = 0; k < kNumStepResidency; k++)
+        if (kStepResidency[k] == cfg->warps_per_sm) r = k;
+    if (r < 0 || (r > 0 && !cfg->persistent))
+        return fail(h, RSB_ERR_INVALID, "rsb_set_step_config: warps_per_sm must be 0, 1, 2, 3, 4 or 6 (persistent only)");
     for (int v = 0; v < kNumStepVariants; v++)
         for (int b = 0; b < kNumStepBlocks; b++)
             if (kStepVariants[v].minBlocks == cfg->min_blocks && kStepBlocks[b] == cfg->block &&
                 kStepVariants[v].persistent == (cfg->persistent != 0)) {
                 h->stepVariant = v;
                 h->stepBlock = b;
+                h->stepResidency = r;
                 return RSB_OK;
             }
     return fail(h, RSB_ERR_INVALID, "rsb_set_step_config: no such launch configuration");

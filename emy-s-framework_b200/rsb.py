@@ -152,7 +152,8 @@ def culler_config(**kw) -> CullerConfig:
 
 
 class TuneEntry(C.Structure):
-    _fields_ = [("min_blocks", C.c_int32), ("block", C.c_int32), ("ms", C.c_float), ("persistent", C.c_int32)]
+    _fields_ = [("min_blocks", C.c_int32), ("block", C.c_int32), ("ms", C.c_float), ("persistent", C.c_int32),
+                ("warps_per_sm", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -556,15 +557,16 @@ class Batch:
 
     def autotune(self, ticks: int = 8) -> list[dict]:
         """rsb_autotune: times the step kernel's launch configurations, keeps the fastest."""
-        out = (TuneEntry * 32)()
+        out = (TuneEntry * 64)()
         n = C.c_int32()
-        self._check(self.lib.rsb_autotune(self._h, ticks, out, 32, C.byref(n)))
-        return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms, "persistent": e.persistent}
-                for e in out[:n.value]]
+        self._check(self.lib.rsb_autotune(self._h, ticks, out, 64, C.byref(n)))
+        return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms, "persistent": e.persistent,
+                 "warps_per_sm": e.warps_per_sm} for e in out[:min(n.value, 64)]]
 
-    def set_step_config(self, min_blocks: int, block: int, persistent: bool = False):
+    def set_step_config(self, min_blocks: int, block: int, persistent: bool = False, warps_per_sm: int = 0):
         """rsb_set_step_config: pins a launch configuration of the step kernel."""
-        e = TuneEntry(min_blocks=min_blocks, block=block, ms=0.0, persistent=1 if persistent else 0)
+        e = TuneEntry(min_blocks=min_blocks, block=block, ms=0.0, persistent=1 if persistent else 0,
+                      warps_per_sm=warps_per_sm)
         self._check(self.lib.rsb_set_step_config(self._h, C.byref(e)))
 
     # ---------------------------------------------------------------- learned culler

@@ -71,8 +71,12 @@ def test_repeated_predictions_match_oracle(pkg, oracle_lib, meshes_dir):
             for b in (eng, ora):
                 b.set_balls(balls)
         elif balls == "stepped":
+            # both sides take the stepped balls through the public state (uu): the engine's
+            # records and the oracle's Bullet bodies then hold the same values
             ora.step(8)
-            eng.set_balls(ora.get_balls())
+            stepped = ora.get_balls()
+            for b in (eng, ora):
+                b.set_balls(stepped)
         pe, po = eng.predict_ball(SLICES), ora.predict_ball(SLICES)
         for k, t in enumerate(SLICES):
             d = np.linalg.norm(vec(pe[:, k], "pos") - vec(po[:, k], "pos"), axis=1)

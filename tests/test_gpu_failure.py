@@ -64,31 +64,42 @@ def test_nonfinite_state_is_flagged_and_contained(pkg, meshes_dir):
 def test_wrong_culler_bound_is_caught_by_the_audit(pkg, meshes_dir):
     rsb = pkg.rsb
     n = 256
-    exact, audit = (rsb.Batch(pkg.engine_library(), n, team_size=2, meshes_path=meshes_dir, cull_mode=m)
+    exact, audit = (rsb.Batch(pkg.engine_library(), n, team_size=1, meshes_path=meshes_dir, cull_mode=m)
                     for m in (rsb.RSB_CULL_EXACT, rsb.RSB_CULL_LEARNED_AUDIT))
-    # a network that answers 1e6 uu everywhere (zero weights, output bias 1e6): every bound
+    # a network that answers 1e6 km everywhere (zero weights, output bias 1e6): every bound
     # clears every body's reach
     params = np.zeros(rsb.RSB_CULLER_PARAMS, np.float32)
     params[-1] = 1e6
     audit.culler_set(params, 0.0)
-    lut = rsb.default_action_lut(exact.lib)
+    # cars and balls at mid height, far from the floor, ceiling and side-wall planes (whose
+    # exact distances the culler keeps), flying into a back wall, which is an arena mesh
+    rng = np.random.default_rng(14)
+    cars = random_cars(rsb, exact.get_cars(), seed=15)
+    side = np.where(np.arange(len(cars)) % 2 == 0, 1.0, -1.0)
+    cars["pos"]["x"] = rng.uniform(-2500, 2500, len(cars))
+    cars["pos"]["y"] = side * 5000
+    cars["pos"]["z"] = rng.uniform(900, 1100, len(cars))
+    cars["vel"]["x"], cars["vel"]["y"], cars["vel"]["z"] = 0.0, side * 1800, 0.0
+    cars["is_on_ground"] = 0
+    balls = random_balls(rsb, n, seed=16)
+    balls["pos"]["x"] = rng.uniform(-2500, 2500, n)
+    balls["pos"]["y"] = rng.choice([-4900.0, 4900.0], n)
+    balls["pos"]["z"] = rng.uniform(900, 1100, n)
+    balls["vel"]["x"], balls["vel"]["y"], balls["vel"]["z"] = 0.0, np.sign(balls["pos"]["y"]) * 2500, 0.0
+    ctl = np.zeros(exact.num_cars, rsb.CONTROLS_DTYPE)
     for x in (exact, audit):
-        x.set_action_lut(lut)
-        x.reset_all(11, rsb.RSB_RESET_KICKOFF)
-    rng = np.random.default_rng(12)
-    for _ in range(6):
-        idx = rng.integers(0, rsb.RSB_NUM_ACTIONS, exact.num_cars).astype(np.int32)
-        for x in (exact, audit):
-            x.set_actions(idx)
-            x.step(8)
+        x.set_cars(cars)
+        x.set_balls(balls)
+        x.set_controls(ctl)
+        x.step(8)
+        x.step(8)
     st = audit.stats()
     info = audit.get_arena_info()
     flagged = (info["status"] & rsb.RSB_ARENA_CULL_MISS) != 0
-    assert st["missed_contacts"] > 0
     assert st["culled_queries"] > 0
-    # every arena has cars on the floor at kickoff, so every arena misses a contact
-    assert flagged.all()
-    assert st["arenas_reverted"] == n
+    assert st["missed_contacts"] > 0
+    assert flagged.sum() > n // 2
+    assert st["arenas_reverted"] == int(flagged.sum())
     assert exact.get_cars().tobytes() == audit.get_cars().tobytes()
     assert exact.get_balls().tobytes() == audit.get_balls().tobytes()
     assert exact.get_pads().tobytes() == audit.get_pads().tobytes()

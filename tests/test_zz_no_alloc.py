@@ -35,9 +35,13 @@ def test_static_actions_match_allocating_path_twice(pkg, meshes_dir):
 def test_static_actions_allocate_no_device_memory(pkg, meshes_dir):
     """After the first call on the device (which looks up the array's address), further calls
     leave the device's free memory unchanged."""
+    import gc
+
     import torch
 
-    _, b = _pair(pkg, meshes_dir, 4096, 3)
+    a, b = _pair(pkg, meshes_dir, 4096, 3)
+    a.close()
+    gc.collect()  # batches of earlier tests release their device memory before the window
     rng = np.random.default_rng(12)
     idx = rng.integers(0, pkg.rsb.RSB_NUM_ACTIONS, b.num_cars).astype(np.int32)
     b.set_actions_static(idx)

@@ -62,6 +62,7 @@ struct EnvView {
     CtlRec* controls;
     float* obs;
     int stride;
+    const uint16_t* obsSrc;  // [team size 1..3][slot][column] -> offset in the arena's block row
     uint8_t* masks;
     float* rewards;
     uint8_t* terminals;
@@ -107,9 +108,45 @@ constexpr uint32_t OF_GROUND = 1, OF_FLIPJUMP = 2, OF_DEMOED = 4, OF_JUMPED = 8,
 
 // The parts of a row that do not depend on the viewing player itself, built once per arena:
 // the ball block and every car's 29-value block, in each team's frame (orange = InvertPhys).
+// A row is a gather from the arena's block row: ball (per frame), pad values (per frame), the
+// cars' actions, the car blocks, and a zero for the padding of smaller arenas.
 constexpr int OB_BALL = 0;                      // [frame][9]
-constexpr int OB_CAR = 2 * 9;                   // [frame][car][29]
-constexpr int OB_WORDS = OB_CAR + 2 * MAX_CARS * 29 + 1;  // odd row stride: fewer bank conflicts
+constexpr int OB_PAD = OB_BALL + 2 * 9;         // [frame][34]
+constexpr int OB_PREV = OB_PAD + 2 * NUM_PADS;  // [car][8]
+constexpr int OB_CAR = OB_PREV + MAX_CARS * 8;  // [frame][car][29]
+constexpr int OB_ZERO = OB_CAR + 2 * MAX_CARS * 29;
+constexpr int OB_WORDS = OB_ZERO + 1;           // odd row stride: fewer bank conflicts
+
+// Offset in the block row of column `col` of the observation row of slot p in an arena of
+// team size T (AdvancedObs.cpp:25-65 with the teammate / opponent order described above):
+// built once on the host for the batch's row stride.
+inline int obsSource(int T, int p, int col) {
+    if (p >= 2 * T) return OB_ZERO;
+    const bool orange = p >= T;
+    if (col < 9) return OB_BALL + (orange ? 9 : 0) + col;
+    if (col < 17) return OB_PREV + p * 8 + (col - 9);
+    if (col < 51) return OB_PAD + (orange ? NUM_PADS : 0) + (col - 17);
+    const int k = (col - 51) / 29, j = (col - 51) - 29 * k;
+    if (k >= 2 * T) return OB_ZERO;
+    int q;
+    const int ownFirst = orange ? T : 0, oppFirst = orange ? 0 : T;
+    if (k == 0) {
+        q = p;
+    } else if (k < T) {
+        // teammates, descending slot order, skipping the player
+        q = ownFirst + T - 1 - (k - 1);
+        if (q <= p) q--;
+    } else {
+        q = oppFirst + T - 1 - (k - T);
+    }
+    return OB_CAR + ((orange ? MAX_CARS : 0) + q) * 29 + j;
+}
+inline void obsSourceTable(int stride, uint16_t* tab) {
+    for (int T = 1; T <= RSB_MAX_TEAM_SIZE; T++)
+        for (int p = 0; p < MAX_CARS; p++)
+            for (int col = 0; col < stride; col++)
+                tab[((T - 1) * MAX_CARS + p) * stride + col] = (uint16_t)obsSource(T, p, col);
+}
 
 struct ObsShared {
     float in[OI_WORDS][OBS_ARENAS];
@@ -157,29 +194,6 @@ RSB_D float obsCarValue(const ObsShared& S, int la, int q, bool inv, int j) {
     if (j == 26) return (f & OF_FLIPJUMP) ? 1.f : 0.f;
     if (j == 27) return (f & OF_DEMOED) ? 1.f : 0.f;
     return (f & OF_JUMPED) ? 1.f : 0.f;
-}
-
-// Element `col` of the observation row of slot p in local arena la, from the built blocks.
-RSB_D float obsValue(const ObsShared& S, int la, int p, int col) {
-    const int T = (int)S.in[OI_TEAM][la];
-    const bool orange = p >= T;
-    if (col < 9) return S.blk[la][OB_BALL + (orange ? 9 : 0) + col];
-    if (col < 17) return S.in[OI_PREV + p * 8 + (col - 9)][la];
-    if (col < 51) return S.in[OI_PAD + (orange ? NUM_PADS : 0) + (col - 17)][la];
-    const int k = (col - 51) / 29, j = (col - 51) - 29 * k;
-    if (k >= 2 * T) return 0.f;  // rows of smaller arenas in a ragged batch are zero-padded
-    int q;
-    const int ownFirst = orange ? T : 0, oppFirst = orange ? 0 : T;
-    if (k == 0) {
-        q = p;
-    } else if (k < T) {
-        // teammates, descending slot order, skipping the player
-        q = ownFirst + T - 1 - (k - 1);
-        if (q <= p) q--;
-    } else {
-        q = oppFirst + T - 1 - (k - T);
-    }
-    return S.blk[la][OB_CAR + ((orange ? MAX_CARS : 0) + q) * 29 + j];
 }
 
 // A block serves 16 arenas in three phases, every thread taking part in each:
@@ -272,19 +286,23 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
     }
     __syncthreads();
 
-    // ---- B: ball blocks and car blocks of both frames
-    constexpr int PER_ARENA = 2 * 9 + 2 * MAX_CARS * 29;
-    for (int i = tid; i < PER_ARENA * OBS_ARENAS; i += OBS_THREADS) {
+    // ---- B: the block row of every arena (ball and car blocks of both frames, pad values of
+    // both frames, the actions, a zero)
+    for (int i = tid; i < OB_WORDS * OBS_ARENAS; i += OBS_THREADS) {
         const int la = i % OBS_ARENAS, w = i / OBS_ARENAS;
         if (la >= na) continue;
         float v = 0.f;
-        if (w < 18) {
+        if (w < OB_PAD) {
             const int col = w % 9;
             const bool orange = w >= 9;
             v = S.in[OI_BALL + col][la] * (col < 3 ? OBS_POS : (col < 6 ? OBS_VEL : OBS_ANG));
             if (orange && (col % 3) < 2) v = -v;
-        } else {
-            const int c = w - 18, fq = c / 29, j = c - 29 * fq;
+        } else if (w < OB_PREV) {
+            v = S.in[OI_PAD + (w - OB_PAD)][la];
+        } else if (w < OB_CAR) {
+            v = S.in[OI_PREV + (w - OB_PREV)][la];
+        } else if (w < OB_ZERO) {
+            const int c = w - OB_CAR, fq = c / 29, j = c - 29 * fq;
             const int q = fq % MAX_CARS;
             if (q < 2 * (int)S.in[OI_TEAM][la]) v = obsCarValue(S, la, q, fq >= MAX_CARS, j);
         }
@@ -292,33 +310,29 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
     }
     __syncthreads();
 
-    // ---- C: the rows (contiguous for the block's arenas), then the masks
+    // ---- C: the rows (contiguous for the block's arenas), then the masks.  Each warp writes
+    // one contiguous stretch, its lanes on consecutive elements: a coalesced 128-byte store
+    // per warp instruction, and consecutive shared-memory words for consecutive lanes.
     const int rows = E.carOffset[a0 + na] - row0;
     const int stride = E.stride;
     float* out = E.obs + (size_t)row0 * stride;
     const int n = rows * stride;
-    auto elem = [&](int e) {
-        const int r = e / stride, col = e - r * stride;
-        const uint16_t ro = S.rowOf[r];
-        return obsValue(S, ro & 0xff, ro >> 8, col);
-    };
-    // elements before the first 16-byte boundary, whole float4s, then the tail
-    const int head = min(n, (int)(((16 - ((uintptr_t)out & 15)) & 15) / 4));
-    const int body = (n - head) / 4;
-    if (tid < head) out[tid] = elem(tid);
-    float4* out4 = reinterpret_cast<float4*>(out + head);
-    for (int v = tid; v < body; v += OBS_THREADS) {
-        const int e = head + 4 * v;
+    {
+        constexpr int WARPS = OBS_THREADS / 32;
+        const int lane = tid & 31, warp = tid >> 5;
+        const int span = ((n + WARPS - 1) / WARPS + 31) & ~31;
+        const int e0 = warp * span, e1 = min(n, e0 + span);
+        int e = e0 + lane;
         int r = e / stride, col = e - r * stride;
-        float x[4];
-        for (int t = 0; t < 4; t++) {
+        for (; e < e1; e += 32) {
             const uint16_t ro = S.rowOf[r];
-            x[t] = obsValue(S, ro & 0xff, ro >> 8, col);
-            if (++col == stride) { col = 0; r++; }
+            const int la = ro & 0xff, p = ro >> 8;
+            const int T = (int)S.in[OI_TEAM][la];
+            out[e] = S.blk[la][__ldg(&E.obsSrc[((T - 1) * MAX_CARS + p) * stride + col])];
+            col += 32;
+            while (col >= stride) { col -= stride; r++; }
         }
-        out4[v] = make_float4(x[0], x[1], x[2], x[3]);
     }
-    for (int e = head + 4 * body + tid; e < n; e += OBS_THREADS) out[e] = elem(e);
     // masks: rows * 90 bytes, 4-byte aligned (every arena has an even number of cars)
     uint32_t* mout = reinterpret_cast<uint32_t*>(E.masks + (size_t)row0 * RSB_NUM_ACTIONS);
     const int nw = rows * RSB_NUM_ACTIONS / 4;

@@ -518,6 +518,9 @@ def reference_gpu(batch, wl, lut, meshes, steps, warmup, settle):
     lib.rscref_time_env_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
                                           C.POINTER(C.c_float)]
     lib.rscref_positions.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rscref_step.restype = lib.rscref_cars_ground.restype = C.c_int32
+    lib.rscref_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.rscref_cars_ground.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     t0 = time.perf_counter()
     h = lib.rscref_create(wl.num_arenas, wl.team_size, meshes.encode())
     if not h:
@@ -537,13 +540,102 @@ def reference_gpu(batch, wl, lut, meshes, steps, warmup, settle):
         bp = np.zeros((wl.num_arenas, 3), np.float32)
         lib.rscref_positions(h, cp.ctypes.data, bp.ctypes.data)
         value = wl.num_arenas * wl.tick_skip * steps / (ms.value / 1e3)
-        return {"value": value, "unit": "arena-ticks/s", "ms_per_step": ms.value / steps, "steps": steps,
+        lib.rscref_destroy(h)
+        h = None
+        drift = reference_gpu_drift(load_pkg(), lib, meshes)
+        return {"value": value, "drift_vs_reference_cpu": drift, "unit": "arena-ticks/s", "ms_per_step": ms.value / steps, "steps": steps,
                 "warmup": warmup, "setup_s": setup_s, "finite_state": bool(np.isfinite(cp).all() and
                                                                           np.isfinite(bp).all()),
                 "kernel": "RocketSimCuda stepArenaKernel + env kernels (reference sources, sm_100a)",
                 "start": f"its kickoff reset, {settle} settle + {warmup - settle} warm-up env steps; seeded uniform actions"}
     finally:
+        if h:
+            lib.rscref_destroy(h)
+
+
+def reference_gpu_drift(pkg, lib, meshes, n=256, ticks=120, seed=0x5EED0006):
+    """What the reference GPU batch trades for its speed: it and the engine run `ticks` single
+    ticks beside the reference CPU RocketSim (the oracle) from identical car and ball states
+    (cars on the ground at random places, headings and speeds; balls anywhere) with the same
+    controls, redrawn every 8 ticks.  Reported: car position drift from the CPU reference at
+    the end (median, 99th percentile, uu) and the share of car-ticks whose on-ground flag
+    differs, for the reference GPU batch and for the engine.  Arenas whose cars the CPU
+    reference visits in another order than the engine are left out of the engine's figures."""
+    import ctypes as C
+
+    rsb = pkg.rsb
+    ora = rsb.Batch(rsb.load_library(ORACLE_LIB), n, team_size=3, meshes_path=meshes, threads=8)
+    eng = rsb.Batch(pkg.engine_library(), n, team_size=3, meshes_path=meshes)
+    h = lib.rscref_create(n, 3, meshes.encode())
+    if not h:
+        return {"unavailable": "the reference batch could not be created"}
+    try:
+        rng = np.random.default_rng(seed)
+        cars = ora.get_cars()
+        m = len(cars)
+        yaw = rng.uniform(-np.pi, np.pi, m)
+        cy, sy = np.cos(yaw), np.sin(yaw)
+        cars["pos"]["x"], cars["pos"]["y"], cars["pos"]["z"] = rng.uniform(-3500, 3500, m), rng.uniform(-4500, 4500, m), 17.0
+        for f, v in (("forward", (cy, sy, 0 * cy)), ("right", (-sy, cy, 0 * cy)), ("up", (0 * cy, 0 * cy, 1 + 0 * cy))):
+            for k, comp in enumerate("xyz"):
+                cars["rot"][f][comp] = v[k]
+        sp = rng.uniform(0, 2300, m)
+        cars["vel"]["x"], cars["vel"]["y"], cars["vel"]["z"] = cy * sp, sy * sp, 0.0
+        cars["boost"] = rng.uniform(0, 100, m)
+        cars["is_on_ground"] = 1
+        balls = np.zeros(n, rsb.BALL_DTYPE)
+        for k, f in enumerate(("forward", "right", "up")):
+            balls["rot"][f]["xyz"[k]] = 1.0
+        balls["pos"]["x"], balls["pos"]["y"], balls["pos"]["z"] = (rng.uniform(-3900, 3900, n), rng.uniform(-5000, 5000, n),
+                                                                  rng.uniform(100, 1900, n))
+        for c in "xyz":
+            balls["vel"][c] = rng.uniform(-3000, 3000, n)
+        for b in (ora, eng):
+            b.set_cars(cars)
+            b.set_balls(balls)
+        if lib.rscref_set_states(h, cars.ctypes.data, balls.ctypes.data):
+            return {"unavailable": "setting the reference batch's states failed"}
+        order = np.zeros(n, bool)
+        fn = ora.lib.rsbref_car_order
+        fn.restype, fn.argtypes = C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p]
+        buf = np.zeros(8, np.int32)
+        for a in range(n):
+            k = fn(ora._h, a, buf.ctypes.data)
+            order[a] = k >= 0 and np.array_equal(buf[:k], np.arange(k)[::-1])
+        keep = np.repeat(order, 6)
+        cp = np.zeros((m, 3), np.float32)
+        gr = np.zeros(m, np.uint8)
+        bp = np.zeros((n, 3), np.float32)
+        flag_ref = flag_eng = 0
+        for t in range(ticks):
+            if t % 8 == 0:
+                ctl = np.zeros(m, rsb.CONTROLS_DTYPE)
+                for f in ("throttle", "steer", "pitch", "yaw", "roll"):
+                    ctl[f] = rng.integers(-1, 2, m).astype(np.float32)
+                ctl["jump"], ctl["boost"], ctl["handbrake"] = rng.random(m) < 0.2, rng.random(m) < 0.4, rng.random(m) < 0.15
+                ora.set_controls(ctl)
+                eng.set_controls(ctl)
+            ora.step(1)
+            eng.step(1)
+            if lib.rscref_step(h, ctl.ctypes.data, 1):
+                return {"unavailable": "the reference batch's step reported a CUDA error"}
+            oc, ec = ora.get_cars(), eng.get_cars()
+            lib.rscref_cars_ground(h, cp.ctypes.data, gr.ctypes.data, bp.ctypes.data)
+            flag_ref += int((gr != oc["is_on_ground"]).sum())
+            flag_eng += int((ec["is_on_ground"] != oc["is_on_ground"])[keep].sum())
+        opos = np.stack([oc["pos"][k] for k in "xyz"], 1).astype(np.float64)
+        epos = np.stack([ec["pos"][k] for k in "xyz"], 1).astype(np.float64)
+        d_ref = np.linalg.norm(cp - opos, axis=1)
+        d_eng = np.linalg.norm(epos - opos, axis=1)[keep]
+        return {"arenas": n, "team_size": 3, "ticks": ticks,
+                "reference_gpu": {"drift_median_uu": float(np.median(d_ref)), "drift_p99_uu": float(np.percentile(d_ref, 99)),
+                                  "on_ground_mismatch": flag_ref / (m * ticks)},
+                "engine": {"drift_median_uu": float(np.median(d_eng)), "drift_p99_uu": float(np.percentile(d_eng, 99)),
+                           "on_ground_mismatch": flag_eng / (int(keep.sum()) * ticks), "arenas": int(order.sum())}}
+    finally:
         lib.rscref_destroy(h)
+        ora.close()
+        eng.close()
 
 
 def stress_events(pkg, trained, wl, rank, dev):

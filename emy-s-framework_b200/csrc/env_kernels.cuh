@@ -286,27 +286,32 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
     }
     __syncthreads();
 
-    // ---- B: the block row of every arena (ball and car blocks of both frames, pad values of
-    // both frames, the actions, a zero)
-    for (int i = tid; i < OB_WORDS * OBS_ARENAS; i += OBS_THREADS) {
+    // ---- B: the block row of every arena: ball, pad values and actions copied per frame,
+    // then one thread per (arena, car) writes that car's 29-value block in both frames
+    for (int i = tid; i < OB_CAR * OBS_ARENAS; i += OBS_THREADS) {
         const int la = i % OBS_ARENAS, w = i / OBS_ARENAS;
         if (la >= na) continue;
-        float v = 0.f;
+        float v;
         if (w < OB_PAD) {
             const int col = w % 9;
-            const bool orange = w >= 9;
             v = S.in[OI_BALL + col][la] * (col < 3 ? OBS_POS : (col < 6 ? OBS_VEL : OBS_ANG));
-            if (orange && (col % 3) < 2) v = -v;
+            if (w >= 9 && (col % 3) < 2) v = -v;
         } else if (w < OB_PREV) {
             v = S.in[OI_PAD + (w - OB_PAD)][la];
-        } else if (w < OB_CAR) {
+        } else {
             v = S.in[OI_PREV + (w - OB_PREV)][la];
-        } else if (w < OB_ZERO) {
-            const int c = w - OB_CAR, fq = c / 29, j = c - 29 * fq;
-            const int q = fq % MAX_CARS;
-            if (q < 2 * (int)S.in[OI_TEAM][la]) v = obsCarValue(S, la, q, fq >= MAX_CARS, j);
         }
         S.blk[la][w] = v;
+    }
+    for (int i = tid; i < MAX_CARS * OBS_ARENAS; i += OBS_THREADS) {
+        const int la = i % OBS_ARENAS, q = i / OBS_ARENAS;
+        if (la >= na) continue;
+        S.blk[la][OB_ZERO] = 0.f;
+        const bool live = q < 2 * (int)S.in[OI_TEAM][la];
+        for (int f = 0; f < 2; f++) {
+            float* o = &S.blk[la][OB_CAR + (f * MAX_CARS + q) * 29];
+            for (int j = 0; j < 29; j++) o[j] = live ? obsCarValue(S, la, q, f == 1, j) : 0.f;
+        }
     }
     __syncthreads();
 
@@ -324,11 +329,18 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
         const int e0 = warp * span, e1 = min(n, e0 + span);
         int e = e0 + lane;
         int r = e / stride, col = e - r * stride;
+        const float* blk = nullptr;
+        const uint16_t* src = nullptr;
+        int rowDone = -1;
         for (; e < e1; e += 32) {
-            const uint16_t ro = S.rowOf[r];
-            const int la = ro & 0xff, p = ro >> 8;
-            const int T = (int)S.in[OI_TEAM][la];
-            out[e] = S.blk[la][__ldg(&E.obsSrc[((T - 1) * MAX_CARS + p) * stride + col])];
+            if (r != rowDone) {  // this lane's row changed: its arena's block row and column map
+                const uint16_t ro = S.rowOf[r];
+                const int la = ro & 0xff, p = ro >> 8;
+                blk = S.blk[la];
+                src = E.obsSrc + (((int)S.in[OI_TEAM][la] - 1) * MAX_CARS + p) * stride;
+                rowDone = r;
+            }
+            out[e] = blk[__ldg(src + col)];
             col += 32;
             while (col >= stride) { col -= stride; r++; }
         }

@@ -142,6 +142,43 @@ int32_t rscref_time_env_steps(void* h, const int32_t* actions, int32_t warmup, i
     return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+// SetAllCarControls with rsb_controls, then Step(ticks), synchronously.
+int32_t rscref_step(void* h, const rsb_controls* ctl, int32_t ticks) {
+    RefGpu* r = static_cast<RefGpu*>(h);
+    if (!r || !ctl || ticks <= 0) return -1;
+    std::vector<rsc::CarControls> c((size_t)r->n * r->carsPerArena);
+    for (size_t i = 0; i < c.size(); i++) {
+        c[i].throttle = ctl[i].throttle;
+        c[i].steer = ctl[i].steer;
+        c[i].pitch = ctl[i].pitch;
+        c[i].yaw = ctl[i].yaw;
+        c[i].roll = ctl[i].roll;
+        c[i].jump = ctl[i].jump != 0;
+        c[i].boost = ctl[i].boost != 0;
+        c[i].handbrake = ctl[i].handbrake != 0;
+    }
+    r->batch.SetKernelSync(true);
+    r->batch.SetAllCarControls(c.data());
+    r->batch.Step(ticks);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// Positions (x, y, z) and on-ground flags of every car, positions of every ball.
+int32_t rscref_cars_ground(void* h, float* car_xyz, uint8_t* on_ground, float* ball_xyz) {
+    RefGpu* r = static_cast<RefGpu*>(h);
+    if (!r || !car_xyz || !on_ground || !ball_xyz) return -1;
+    std::vector<rsc::CarState> cs((size_t)r->n * r->carsPerArena);
+    std::vector<rsc::BallState> bs((size_t)r->n);
+    r->batch.GetAllCarStates(cs.data());
+    r->batch.GetAllBallStates(bs.data());
+    for (size_t i = 0; i < cs.size(); i++) {
+        std::memcpy(car_xyz + 3 * i, &cs[i].pos, 12);
+        on_ground[i] = cs[i].isOnGround ? 1 : 0;
+    }
+    for (size_t i = 0; i < bs.size(); i++) std::memcpy(ball_xyz + 3 * i, &bs[i].pos, 12);
+    return 0;
+}
+
 // Positions of every car (x, y, z per car) and ball, to check the comparator ran.
 int32_t rscref_positions(void* h, float* car_xyz, float* ball_xyz) {
     RefGpu* r = static_cast<RefGpu*>(h);

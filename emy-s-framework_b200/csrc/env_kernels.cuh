@@ -94,7 +94,7 @@ RSB_D float vdot4(float ax, float ay, float az, float bx, float by, float bz) {
 // ------------------------------------------------------------------ observations
 
 // Per-arena inputs staged in shared memory, one column per arena of the block.
-constexpr int OBS_ARENAS = 16;
+constexpr int OBS_ARENAS = 8;
 constexpr int OI_BALL = 0;                                   // pos, vel, ang (uu)
 constexpr int OI_CAR = 9;                                    // per car, OI_CAR_N words
 constexpr int OI_CAR_N = 20;                                 // pos vel ang fwd right up boost flags
@@ -196,13 +196,14 @@ RSB_D float obsCarValue(const ObsShared& S, int la, int q, bool inv, int j) {
     return (f & OF_JUMPED) ? 1.f : 0.f;
 }
 
-// A block serves 16 arenas in three phases, every thread taking part in each:
+// A block serves 8 arenas (24 KB of shared memory, so that 9 blocks share an SM and overlap
+// their phases) in three phases, every thread taking part in each:
 //   A. stage the arenas' records from the word planes (consecutive threads read consecutive
 //      arenas of one word: coalesced), derive flags, masks, pad values and the actions;
 //   B. build the ball block and the 29-value block of every car once per team frame;
 //   C. write the arenas' rows, which are contiguous in the output, as 16-byte stores of four
 //      elements assembled from the blocks, and the mask bytes as 32-bit words.
-constexpr int OBS_THREADS = 256;
+constexpr int OBS_THREADS = 128;
 __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb) {
     __shared__ ObsShared S;
     const int tid = threadIdx.x;

@@ -160,40 +160,41 @@ struct ObsShared {
     uint16_t rowOf[OBS_ARENAS * MAX_CARS];   // local row -> arena (low byte) | slot << 8
 };
 
-RSB_D float obsCarValue(const ObsShared& S, int la, int q, bool inv, int j) {
-    const int o = OI_CAR + q * OI_CAR_N;
-    auto g = [&](int k) { return S.in[o + k][la]; };
-    // InvertPhys: x and y of every vector negated
-    auto iv = [&](int k, int comp) { float v = g(k + comp); return (inv && comp < 2) ? -v : v; };
-    if (j < 3) return iv(0, j) * OBS_POS;
-    if (j < 6) return iv(9, j - 3);
-    if (j < 9) return iv(15, j - 6);
-    if (j < 12) return iv(3, j - 9) * OBS_VEL;
-    if (j < 15) return iv(6, j - 12) * OBS_ANG;
-    if (j < 24) {
-        // rotMat.Dot(v) = (v.forward, v.right, v.up)
-        int r = (j - 15) % 3, kind = (j - 15) / 3;
-        int bk = 9 + 3 * r;
-        float bx = iv(bk, 0), by = iv(bk, 1), bz = iv(bk, 2);
-        float vx, vy, vz, coef;
-        if (kind == 0) {
-            vx = iv(6, 0); vy = iv(6, 1); vz = iv(6, 2);
-            coef = OBS_ANG;
-        } else {
-            int bo = kind == 1 ? 0 : 3;  // ball pos / vel in the staged ball block
-            float cx = S.in[OI_BALL + bo + 0][la], cy = S.in[OI_BALL + bo + 1][la], cz = S.in[OI_BALL + bo + 2][la];
-            if (inv) { cx = -cx; cy = -cy; }
-            vx = cx - iv(bo, 0); vy = cy - iv(bo, 1); vz = cz - iv(bo, 2);
-            coef = kind == 1 ? OBS_POS : OBS_VEL;
-        }
-        return vdot4(vx, vy, vz, bx, by, bz) * coef;
+// The 29 values of car q's block in one frame (inv: the orange frame, InvertPhys), written to
+// o[0..29) (AdvancedObs::AddPlayerToObs, AdvancedObs.cpp:25-49: position, forward, up,
+// velocity, angular velocity, the three rotMat.Dot rows, boost, four flags).
+RSB_D void obsCarBlock(const ObsShared& S, int la, int q, bool inv, float* o) {
+    const int b = OI_CAR + q * OI_CAR_N;
+    float g[18];
+    for (int k = 0; k < 18; k++) g[k] = S.in[b + k][la];
+    if (inv)
+        for (int k = 0; k < 18; k += 3) { g[k] = -g[k]; g[k + 1] = -g[k + 1]; }
+    // pos 0..2, vel 3..5, ang 6..8, forward 9..11, right 12..14, up 15..17
+    o[0] = g[0] * OBS_POS; o[1] = g[1] * OBS_POS; o[2] = g[2] * OBS_POS;
+    o[3] = g[9]; o[4] = g[10]; o[5] = g[11];
+    o[6] = g[15]; o[7] = g[16]; o[8] = g[17];
+    o[9] = g[3] * OBS_VEL; o[10] = g[4] * OBS_VEL; o[11] = g[5] * OBS_VEL;
+    o[12] = g[6] * OBS_ANG; o[13] = g[7] * OBS_ANG; o[14] = g[8] * OBS_ANG;
+    float bp[3], bv[3];
+    for (int k = 0; k < 3; k++) {
+        bp[k] = S.in[OI_BALL + k][la];
+        bv[k] = S.in[OI_BALL + 3 + k][la];
     }
-    if (j == 24) return g(18) / 100.f;
-    uint32_t f = __float_as_uint(g(19));
-    if (j == 25) return (f & OF_GROUND) ? 1.f : 0.f;
-    if (j == 26) return (f & OF_FLIPJUMP) ? 1.f : 0.f;
-    if (j == 27) return (f & OF_DEMOED) ? 1.f : 0.f;
-    return (f & OF_JUMPED) ? 1.f : 0.f;
+    if (inv) { bp[0] = -bp[0]; bp[1] = -bp[1]; bv[0] = -bv[0]; bv[1] = -bv[1]; }
+    const float rp[3] = {bp[0] - g[0], bp[1] - g[1], bp[2] - g[2]};
+    const float rv[3] = {bv[0] - g[3], bv[1] - g[4], bv[2] - g[5]};
+    for (int r = 0; r < 3; r++) {
+        const float* bk = g + 9 + 3 * r;  // forward, right, up
+        o[15 + r] = vdot4(g[6], g[7], g[8], bk[0], bk[1], bk[2]) * OBS_ANG;
+        o[18 + r] = vdot4(rp[0], rp[1], rp[2], bk[0], bk[1], bk[2]) * OBS_POS;
+        o[21 + r] = vdot4(rv[0], rv[1], rv[2], bk[0], bk[1], bk[2]) * OBS_VEL;
+    }
+    o[24] = S.in[b + 18][la] / 100.f;
+    const uint32_t f = __float_as_uint(S.in[b + 19][la]);
+    o[25] = (f & OF_GROUND) ? 1.f : 0.f;
+    o[26] = (f & OF_FLIPJUMP) ? 1.f : 0.f;
+    o[27] = (f & OF_DEMOED) ? 1.f : 0.f;
+    o[28] = (f & OF_JUMPED) ? 1.f : 0.f;
 }
 
 // A block serves 8 arenas (24 KB of shared memory, so that 9 blocks share an SM and overlap
@@ -311,7 +312,9 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
         const bool live = q < 2 * (int)S.in[OI_TEAM][la];
         for (int f = 0; f < 2; f++) {
             float* o = &S.blk[la][OB_CAR + (f * MAX_CARS + q) * 29];
-            for (int j = 0; j < 29; j++) o[j] = live ? obsCarValue(S, la, q, f == 1, j) : 0.f;
+            if (live) obsCarBlock(S, la, q, f == 1, o);
+            else
+                for (int j = 0; j < 29; j++) o[j] = 0.f;
         }
     }
     __syncthreads();
@@ -322,28 +325,16 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
     const int rows = E.carOffset[a0 + na] - row0;
     const int stride = E.stride;
     float* out = E.obs + (size_t)row0 * stride;
-    const int n = rows * stride;
     {
-        constexpr int WARPS = OBS_THREADS / 32;
-        const int lane = tid & 31, warp = tid >> 5;
-        const int span = ((n + WARPS - 1) / WARPS + 31) & ~31;
-        const int e0 = warp * span, e1 = min(n, e0 + span);
-        int e = e0 + lane;
-        int r = e / stride, col = e - r * stride;
-        const float* blk = nullptr;
-        const uint16_t* src = nullptr;
-        int rowDone = -1;
-        for (; e < e1; e += 32) {
-            if (r != rowDone) {  // this lane's row changed: its arena's block row and column map
-                const uint16_t ro = S.rowOf[r];
-                const int la = ro & 0xff, p = ro >> 8;
-                blk = S.blk[la];
-                src = E.obsSrc + (((int)S.in[OI_TEAM][la] - 1) * MAX_CARS + p) * stride;
-                rowDone = r;
-            }
-            out[e] = blk[__ldg(src + col)];
-            col += 32;
-            while (col >= stride) { col -= stride; r++; }
+        // one warp per row, its lanes on consecutive columns
+        const int lane = tid & 31;
+        for (int r = tid >> 5; r < rows; r += OBS_THREADS / 32) {
+            const uint16_t ro = S.rowOf[r];
+            const int la = ro & 0xff, p = ro >> 8;
+            const float* blk = S.blk[la];
+            const uint16_t* src = E.obsSrc + (((int)S.in[OI_TEAM][la] - 1) * MAX_CARS + p) * stride;
+            float* o = out + (size_t)r * stride;
+            for (int col = lane; col < stride; col += 32) o[col] = blk[__ldg(src + col)];
         }
     }
     // masks: rows * 90 bytes, 4-byte aligned (every arena has an even number of cars)

@@ -138,39 +138,7 @@ RSB_HD RaySetup raySetup(V3 src, V3 dst) {
     return r;
 }
 
-// Whether candidate `key` passes the leaf tests of the BVH walk, and then the distance at
-// which the segment crosses its triangle inside the edge tolerance of
-// btTriangleRaycastCallback::processTriangle (the same arithmetic as rayTriangle, without
-// the closest-hit gate).  Returns false when the triangle would not be reported.
-RSB_HD bool rayVoxCandidate(const ArenaStatic& S, uint32_t key, const RaySetup& R, float& distance) {
-    const int m = (int)(key >> 22), leaf = (int)((key >> 10) & 0xFFFu), tri = (int)(key & 0x3FFu);
-    const MeshDesc& md = S.meshes[m];
-    uint16_t qmn[3], qmx[3];
-    bvhQuantizeClamp(md, R.rmn, 0, qmn);
-    bvhQuantizeClamp(md, R.rmx, 1, qmx);
-    const BvhNode& nd = S.nodes[md.nodeOff + leaf];
-    if (!qOverlap(qmn, qmx, nd.qmin, nd.qmax)) return false;
-    V3 bounds[2];
-    bounds[0] = bvhUnquantize(md, nd.qmin);
-    bounds[1] = bvhUnquantize(md, nd.qmax);
-    float param = 1.f;
-    if (!rayAabb2(R.src, R.inv, R.sign, bounds, param, 0.f, R.lambdaMax)) return false;
-    V3 t[3];
-    triVerts(S, m, tri, t);
-    const V3 v10 = t[1] - t[0], v20 = t[2] - t[0];
-    const V3 n = cross(v10, v20);
-    const float dist = dot(t[0], n);
-    const float da = dot(n, R.src) - dist, db = dot(n, R.dst) - dist;
-    if (da * db >= 0.f) return false;
-    distance = da / (da - db);
-    const float edgeTol = length2(n) * -0.0001f;
-    const V3 point = R.src * (1.f - distance) + R.dst * distance;
-    const V3 v0p = t[0] - point, v1p = t[1] - point, v2p = t[2] - point;
-    return dot(cross(v0p, v1p), n) >= edgeTol && dot(cross(v1p, v2p), n) >= edgeTol &&
-           dot(cross(v2p, v0p), n) >= edgeTol;
-}
-
-// One lane's voxel-list query, candidate after candidate (the reference's visiting order).
+// The voxel-list query, candidate after candidate (the reference's visiting order).
 RSB_HD bool rayVsMeshesVoxSerial(const ArenaStatic& S, uint32_t meshes, V3 src, V3 dst, float tol, RayHit& hit,
                                  uint32_t* cand) {
     int nc;
@@ -203,89 +171,7 @@ RSB_HD bool rayVsMeshesVoxSerial(const ArenaStatic& S, uint32_t meshes, V3 src, 
     return true;
 }
 
-struct RayCoopLane {
-    float src[3], dst[3];
-    float cbf;
-    int32_t n, pre;  // candidates (0: not gathered), exclusive prefix over the warp's lanes
-    int32_t pad_;
-    unsigned long long best;  // (distance bits << 32) | candidate index
-};
-constexpr int kRayCoopWarpBytes = 32 * kRayCandidates * 4 + 32 * (int)sizeof(RayCoopLane);
-#if defined(__CUDA_ARCH__)
-// Warp-cooperative form for the step kernels, which give every warp kRayCoopWarpBytes of
-// dynamic shared memory.  The lanes that reach the query together (__activemask) each gather
-// their own candidates into shared memory; then every one of those lanes tests candidates of
-// every query, spread evenly over them, and keeps for each query the minimum of (distance,
-// candidate index) over the triangles the segment crosses closer than the query's current
-// hit.  That minimum is the hit the serial loop ends with: it reports a triangle only when
-// strictly closer than the best so far, so the first of equally close ones wins, and a mesh
-// after an exact (zero) hit could not win either.  The query's own lane then runs
-// rayTriangle on the winner, which sets `hit` bit for bit as the serial loop would.
-extern __shared__ __align__(16) unsigned char g_stepSmem[];
-
-RSB_D bool rayVsMeshesVoxWarp(const ArenaStatic& S, uint32_t meshes, V3 src, V3 dst, float tol, RayHit& hit) {
-    const unsigned mask = __activemask();
-    const int lane = threadIdx.x & 31;
-    unsigned char* base = g_stepSmem + (threadIdx.x >> 5) * kRayCoopWarpBytes;
-    uint32_t* keys = reinterpret_cast<uint32_t*>(base);
-    RayCoopLane* L = reinterpret_cast<RayCoopLane*>(base + 32 * kRayCandidates * 4);
-    int nc = 0;
-    const bool ok = rayVoxGather(S, meshes, src, dst, tol, keys + lane * kRayCandidates, nc);
-    RayCoopLane& me = L[lane];
-    me.src[0] = src.x; me.src[1] = src.y; me.src[2] = src.z;
-    me.dst[0] = dst.x; me.dst[1] = dst.y; me.dst[2] = dst.z;
-    me.cbf = hit.fraction;
-    me.n = ok ? nc : 0;
-    me.best = ~0ull;
-    __syncwarp(mask);
-    int pre = 0;
-    for (int q = 0; q < lane; q++)
-        if ((mask >> q) & 1u) pre += L[q].n;
-    me.pre = pre;
-    __syncwarp(mask);
-    const int nw = __popc(mask), rank = __popc(mask & ((1u << lane) - 1u));
-    for (int q = 0; q < 32; q++) {
-        if (!((mask >> q) & 1u)) continue;
-        const int nq = L[q].n;
-        if (nq == 0) continue;
-        const int p0 = L[q].pre;
-        int g = p0 + (rank - p0 % nw + nw) % nw;  // this lane's first work item of query q
-        if (g >= p0 + nq) continue;
-        const RaySetup R = raySetup(V3{L[q].src[0], L[q].src[1], L[q].src[2]}, V3{L[q].dst[0], L[q].dst[1], L[q].dst[2]});
-        const float cbf = L[q].cbf;
-        for (; g < p0 + nq; g += nw) {
-            const int idx = g - p0;
-            float d;
-            if (rayVoxCandidate(S, keys[q * kRayCandidates + idx], R, d) && d < cbf)
-                atomicMin(&L[q].best, ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)idx);
-        }
-    }
-    __syncwarp(mask);
-    if (ok && nc > 0 && me.best != ~0ull) {
-        const uint32_t key = keys[lane * kRayCandidates + (int)(me.best & 0xffffffffu)];
-        const int m = (int)(key >> 22), tri = (int)(key & 0x3FFu);
-        V3 v[3];
-        triVerts(S, m, tri, v);
-        float cbf = hit.fraction;
-        rayTriangle(v, src, dst, m, hit, cbf);
-    }
-    __syncwarp(mask);  // the shared slots are free again
-    return ok;
-}
-
-RSB_D uint32_t dynamicSmemBytes() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
-    return r;
-}
-#endif
-
 RSB_HD bool rayVsMeshesVox(const ArenaStatic& S, uint32_t meshes, V3 src, V3 dst, float tol, RayHit& hit) {
-#if defined(__CUDA_ARCH__)
-    // the step kernels provide the shared slots; any other caller takes the serial form
-    if (dynamicSmemBytes() >= (uint32_t)(((blockDim.x + 31) >> 5) * kRayCoopWarpBytes))
-        return rayVsMeshesVoxWarp(S, meshes, src, dst, tol, hit);
-#endif
     uint32_t cand[kRayCandidates];
     return rayVsMeshesVoxSerial(S, meshes, src, dst, tol, hit, cand);
 }

@@ -133,7 +133,7 @@ struct rsb_handle {
     int stepVariant = 0, stepBlock = 1, stepResidency = 0;
     uint32_t* dScratch = nullptr;   // the autotuner's copy of the arena records
     unsigned int* dWork = nullptr;  // claim counter of the persistent step kernel
-    int persistGrid[16][4] = {};     // resident blocks (all SMs) per persistent variant and block size
+    int persistGrid[8][4] = {};     // resident blocks (all SMs) per persistent variant and block size
     int smCount = 0;
     uint32_t* dStage = nullptr;     // staging of the per-arena getters
     rsb_ball_state* dPred = nullptr;  // ball prediction slices [num_arenas][n_slices]
@@ -173,10 +173,8 @@ static rsb_status cudaFail(rsb_handle* h, const char* what, cudaError_t e) {
 
 // One thread advances one arena.  MINB is the minimum number of 128-thread blocks per SM
 // the compiler must fit, which caps the registers per thread; the autotuner picks the
-// variant and the block size.  COOP copies are launched with the shared slots of the
-// warp-cooperative mesh-ray queries (phys/ray.h) and a shared-memory carveout for them; the
-// others get no shared memory, keep all of L1 for local memory, and query lane by lane.
-template <int MINB, bool COOP>
+// variant and the block size.
+template <int MINB>
 __global__ void __launch_bounds__(128, MINB) stepKernel(EngineView D, int ticks) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= D.N) return;
@@ -191,7 +189,7 @@ __global__ void __launch_bounds__(128, MINB) stepKernel(EngineView D, int ticks)
 // and the same per-arena computation; the claims pack the work that one-arena-per-thread
 // blocks leave in a partial last wave (65,536 arenas are about 1.7 waves of resident warps).
 // No waiting: a claim is one atomic add.
-template <int MINB, bool COOP>
+template <int MINB>
 __global__ void __launch_bounds__(128, MINB) stepKernelPersistent(EngineView D, int ticks) {
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -213,14 +211,10 @@ struct StepVariant {
     void (*fn)(EngineView, int);
     int minBlocks;
     bool persistent;
-    bool coop;
 };
-static const StepVariant kStepVariants[] = {
-    {stepKernel<1, false>, 1, false, false},          {stepKernel<3, false>, 3, false, false},
-    {stepKernel<4, false>, 4, false, false},          {stepKernelPersistent<1, false>, 1, true, false},
-    {stepKernelPersistent<3, false>, 3, true, false}, {stepKernelPersistent<4, false>, 4, true, false},
-    {stepKernel<1, true>, 1, false, true},            {stepKernel<3, true>, 3, false, true},
-    {stepKernelPersistent<1, true>, 1, true, true},   {stepKernelPersistent<3, true>, 3, true, true}};
+static const StepVariant kStepVariants[] = {{stepKernel<1>, 1, false},          {stepKernel<3>, 3, false},
+                                            {stepKernel<4>, 4, false},          {stepKernelPersistent<1>, 1, true},
+                                            {stepKernelPersistent<3>, 3, true}, {stepKernelPersistent<4>, 4, true}};
 constexpr int kNumStepVariants = sizeof(kStepVariants) / sizeof(kStepVariants[0]);
 static const int kStepBlocks[] = {32, 64, 128};
 constexpr int kNumStepBlocks = sizeof(kStepBlocks) / sizeof(kStepBlocks[0]);
@@ -621,13 +615,7 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
             if (cudaFuncGetAttributes(&fa, v.fn) != cudaSuccess)
                 return fail(nullptr, RSB_ERR_CUDA, "cudaFuncGetAttributes failed");
             need = std::max(need, ((fa.localSizeBytes + 4096) + 1023) / 1024 * 1024);
-            // the rest of L1 for the threads' local memory, but enough shared memory for the
-            // warp-cooperative query slots of every warp that fits on an SM (by registers)
-            const int regs = std::max(1, fa.numRegs);
-            const int warps = std::min(64, 65536 / (regs * 32));
-            const size_t smem = (size_t)warps * (kRayCoopWarpBytes + 1024);
-            const int pct = (int)std::min<size_t>(100, (smem * 100 + 228 * 1024 - 1) / (228 * 1024));
-            cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout, v.coop ? pct : 0);
+            cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
         }
         size_t cur = 0;
         cudaDeviceGetLimit(&cur, cudaLimitStackSize);
@@ -704,12 +692,6 @@ rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride) {
     return RSB_OK;
 }
 
-// Dynamic shared memory of a step-kernel launch: the warp-cooperative mesh-ray queries'
-// candidate slots (phys/ray.h), kRayCoopWarpBytes per warp.
-static size_t stepSmem(const StepVariant& v, int block) {
-    return v.coop ? (size_t)((block + 31) / 32) * kRayCoopWarpBytes : 0;
-}
-
 // Launches step-kernel variant v with block size index b on stream st (a persistent variant
 // first zeroes its claim counter on the same stream).
 static cudaError_t launchStep(rsb_handle* h, const EngineView& D, int v, int b, int ticks, cudaStream_t st,
@@ -721,7 +703,7 @@ static cudaError_t launchStep(rsb_handle* h, const EngineView& D, int v, int b, 
         int& g = h->persistGrid[v][b];
         if (g == 0) {
             int perSm = 0, sms = 0;
-            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sv.fn, block, stepSmem(sv, block));
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sv.fn, block, 0);
             if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
             if (e != cudaSuccess) return e;
             h->smCount = sms;
@@ -736,7 +718,7 @@ static cudaError_t launchStep(rsb_handle* h, const EngineView& D, int v, int b, 
         cudaError_t e = cudaMemsetAsync(h->dWork, 0, sizeof(unsigned int), st);
         if (e != cudaSuccess) return e;
     }
-    sv.fn<<<grid, block, stepSmem(sv, block), st>>>(D, ticks);
+    sv.fn<<<grid, block, 0, st>>>(D, ticks);
     return cudaGetLastError();
 }
 
@@ -816,7 +798,7 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
     for (int v = 0; v < kNumStepVariants; v++)
         for (int b = 0; b < kNumStepBlocks; b++) cands.push_back({v, b, 0});
     for (int v = 0; v < kNumStepVariants; v++)
-        if (kStepVariants[v].persistent && kStepVariants[v].minBlocks == 1 && !kStepVariants[v].coop)
+        if (kStepVariants[v].persistent && kStepVariants[v].minBlocks == 1)
             for (int b = 0; b < 2; b++)
                 for (int r = 1; r < kNumStepResidency; r++) cands.push_back({v, b, r});
     for (const Cand& c : cands) {
@@ -846,8 +828,7 @@ rsb_status rsb_autotune(rsb_handle* h, int32_t ticks, rsb_tune_entry* out, int32
             if (st != RSB_OK) break;
             if (out && n < cap)
                 out[n] = rsb_tune_entry{kStepVariants[v].minBlocks, kStepBlocks[b], ms,
-                                        kStepVariants[v].persistent ? 1 : 0, kStepResidency[c.r],
-                                        kStepVariants[v].coop ? 1 : 0};
+                                        kStepVariants[v].persistent ? 1 : 0, kStepResidency[c.r]};
             n++;
             if (ms < best) { best = ms; bestV = v; bestB = b; bestR = c.r; }
         }
@@ -872,8 +853,7 @@ rsb_status rsb_set_step_config(rsb_handle* h, const rsb_tune_entry* cfg) {
     for (int v = 0; v < kNumStepVariants; v++)
         for (int b = 0; b < kNumStepBlocks; b++)
             if (kStepVariants[v].minBlocks == cfg->min_blocks && kStepBlocks[b] == cfg->block &&
-                kStepVariants[v].persistent == (cfg->persistent != 0) &&
-                kStepVariants[v].coop == (cfg->ray_coop != 0)) {
+                kStepVariants[v].persistent == (cfg->persistent != 0)) {
                 h->stepVariant = v;
                 h->stepBlock = b;
                 h->stepResidency = r;

@@ -153,7 +153,7 @@ def culler_config(**kw) -> CullerConfig:
 
 class TuneEntry(C.Structure):
     _fields_ = [("min_blocks", C.c_int32), ("block", C.c_int32), ("ms", C.c_float), ("persistent", C.c_int32),
-                ("warps_per_sm", C.c_int32), ("ray_coop", C.c_int32)]
+                ("warps_per_sm", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -561,13 +561,12 @@ class Batch:
         n = C.c_int32()
         self._check(self.lib.rsb_autotune(self._h, ticks, out, 64, C.byref(n)))
         return [{"min_blocks": e.min_blocks, "block": e.block, "ms": e.ms, "persistent": e.persistent,
-                 "warps_per_sm": e.warps_per_sm, "ray_coop": e.ray_coop} for e in out[:min(n.value, 64)]]
+                 "warps_per_sm": e.warps_per_sm} for e in out[:min(n.value, 64)]]
 
-    def set_step_config(self, min_blocks: int, block: int, persistent: bool = False, warps_per_sm: int = 0,
-                        ray_coop: bool = False):
+    def set_step_config(self, min_blocks: int, block: int, persistent: bool = False, warps_per_sm: int = 0):
         """rsb_set_step_config: pins a launch configuration of the step kernel."""
         e = TuneEntry(min_blocks=min_blocks, block=block, ms=0.0, persistent=1 if persistent else 0,
-                      warps_per_sm=warps_per_sm, ray_coop=1 if ray_coop else 0)
+                      warps_per_sm=warps_per_sm)
         self._check(self.lib.rsb_set_step_config(self._h, C.byref(e)))
 
     # ---------------------------------------------------------------- learned culler

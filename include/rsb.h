@@ -360,9 +360,6 @@ typedef struct rsb_tune_entry {
     float ms;             /* best of two timed launches of `ticks` ticks */
     int32_t persistent;   /* 1: a grid whose warps claim 32 arenas at a time until none are left */
     int32_t warps_per_sm; /* persistent grids: warps resident per SM (0 = as many as fit) */
-    int32_t ray_coop;     /* 1: the lanes of a warp that reach a wheel ray's mesh query together
-                             test each other's candidate triangles (shared memory per warp);
-                             0: each lane tests its own */
 } rsb_tune_entry;
 
 /* Times every launch configuration of the step kernel on a device copy of the current

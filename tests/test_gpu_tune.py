@@ -23,12 +23,10 @@ def test_autotune_keeps_state_and_results(pkg, meshes_dir):
         x.set_balls(balls)
     before = a.get_cars().tobytes(), a.get_balls().tobytes(), a.get_arena_info().tobytes()
     res = a.autotune(8)
-    # 10 variants (6 lane-by-lane, 4 cooperative) x 3 block sizes at full residency, plus
-    # 2 x 5 residency caps
-    assert len(res) == 40 and all(r["ms"] > 0 for r in res)
-    assert sum(r["persistent"] for r in res) == 25
+    # 6 variants x 3 block sizes at full residency, plus 2 x 5 residency caps
+    assert len(res) == 28 and all(r["ms"] > 0 for r in res)
+    assert sum(r["persistent"] for r in res) == 19
     assert sum(r["warps_per_sm"] > 0 for r in res) == 10
-    assert sum(r["ray_coop"] for r in res) == 12
     assert (a.get_cars().tobytes(), a.get_balls().tobytes(), a.get_arena_info().tobytes()) == before
     ctl = np.zeros(a.num_cars, rsb.CONTROLS_DTYPE)
     ctl["throttle"] = 1
@@ -40,10 +38,8 @@ def test_autotune_keeps_state_and_results(pkg, meshes_dir):
     assert a.get_balls().tobytes() == b.get_balls().tobytes()
 
 
-@pytest.mark.parametrize("min_blocks,block,warps,coop", [(1, 64, 0, False), (3, 32, 0, False), (4, 128, 0, False),
-                                                        (1, 32, 1, False), (1, 64, 3, False), (1, 64, 0, True),
-                                                        (3, 128, 0, True)])
-def test_persistent_launch_is_bit_identical(pkg, meshes_dir, min_blocks, block, warps, coop):
+@pytest.mark.parametrize("min_blocks,block,warps", [(1, 64, 0), (3, 32, 0), (4, 128, 0), (1, 32, 1), (1, 64, 3)])
+def test_persistent_launch_is_bit_identical(pkg, meshes_dir, min_blocks, block, warps):
     """Warps claiming 32 arenas at a time compute every arena exactly as one-thread-per-arena
     blocks do (ragged batch, with an arena count that is not a multiple of 32), at full and at
     capped residency."""
@@ -52,7 +48,7 @@ def test_persistent_launch_is_bit_identical(pkg, meshes_dir, min_blocks, block, 
     n = len(ts)
     a = rsb.Batch(pkg.engine_library(), n, team_sizes=ts, meshes_path=meshes_dir)
     b = rsb.Batch(pkg.engine_library(), n, team_sizes=ts, meshes_path=meshes_dir)
-    a.set_step_config(min_blocks, block, persistent=True, warps_per_sm=warps, ray_coop=coop)
+    a.set_step_config(min_blocks, block, persistent=True, warps_per_sm=warps)
     b.set_step_config(1, 64, persistent=False)
     cars = random_cars(rsb, a.get_cars(), 21)
     balls = random_balls(rsb, n, 22)

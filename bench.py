@@ -311,18 +311,23 @@ def run_ours(args, rank, world, dist):
     start(rsb.RSB_CULL_EXACT)
     warm()
     if wl.graph:
-        # kernel time from a short eager segment, then the env step captured once and replayed
+        # kernel time from a short eager segment, then the library's captured env step
+        # (rsb_env_graph_capture) replayed once per step after the policy's action sampling;
+        # the reset seed advances on the device at every replay
         _, _, kernel_steps, _ = timed(3, [])
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.stream(stream):
-            with torch.cuda.graph(graph, stream=stream):
-                one_step()
-        torch.cuda.synchronize()
-        value, total_ms, _, queries = timed(steps, clocks, graph)
+        batch.env_graph_capture(actions.data_ptr(), wl.tick_skip, reset_mode, 0x5EED2000 + rank)
+
+        class _Replay:
+            @staticmethod
+            def replay():
+                sample_actions()
+                batch.env_graph_launch(stream=sp)
+
+        value, total_ms, _, queries = timed(steps, clocks, _Replay)
         step_times = kernel_steps
-        extra["graph"] = {"launches_per_replay": 6, "note": "reset seeds are fixed inside the captured step"}
+        extra["graph"] = {"api": "rsb_env_graph_capture / rsb_env_graph_launch", "launches_per_replay": 6,
+                          "note": "action sampling (torch) launched outside the graph"}
         ex_value = value
-        del graph
     else:
         value, total_ms, step_times, queries = timed(steps, clocks)
         ex_value, ex_ms, ex_steps, ex_q = value, total_ms, step_times, queries
@@ -340,12 +345,29 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize()
         s1 = batch.stats()
         tested = queries["culled_queries"] + queries["narrowphase_queries"]
+        # the same rollout with the bound that needs no training (voxel distance field)
+        start(rsb.RSB_CULL_VOXEL)
+        warm()
+        vx_value, vx_ms, vx_steps, vx_q = timed(steps, [])
+        start(rsb.RSB_CULL_VOXEL_AUDIT)
+        s2 = batch.stats()
+        with torch.cuda.stream(stream):
+            for _ in range(args.settle + args.warmup + min(steps, 64)):
+                one_step()
+        torch.cuda.synchronize()
+        s3 = batch.stats()
+        vx_tested = vx_q["culled_queries"] + vx_q["narrowphase_queries"]
         learned = {"train": culler, "culled_fraction": queries["culled_queries"] / max(1, tested),
                    "static_tests": queries, "audit_missed_contacts": s1["missed_contacts"] - s0["missed_contacts"],
                    "audit_arenas_reverted": s1["arenas_reverted"],
                    "exact_bvh": {"value": ex_value, "ms_per_step": ex_ms / steps,
                                  "kernel_ms": statistics.mean(ex_steps), "static_tests": ex_q},
-                   "learned_over_exact": value / ex_value}
+                   "learned_over_exact": value / ex_value,
+                   "voxel_bound": {"value": vx_value, "ms_per_step": vx_ms / steps,
+                                   "kernel_ms": statistics.mean(vx_steps),
+                                   "culled_fraction": vx_q["culled_queries"] / max(1, vx_tested),
+                                   "audit_missed_contacts": s3["missed_contacts"] - s2["missed_contacts"],
+                                   "over_exact": vx_value / ex_value}}
         batch.set_cull_mode(rsb.RSB_CULL_LEARNED)
     if wl.preset == "c4":
         extra["stress"] = stress_events(pkg, batch, wl, rank, dev)
@@ -479,7 +501,7 @@ def run_ours(args, rank, world, dist):
         "e2e": {"value": e2e_value, "unit": "arena-ticks/s", "h2d_bytes_per_step": int(statistics.mean(h2d)),
                 "d2h_bytes_per_step": int(statistics.mean(d2h))},
         # per env step: action expansion, (culler,) step, obs + masks, rewards + terminals, reset
-        "gpu_launches": steps * (6 if learned is not None else 5),
+        "gpu_launches": steps * ((6 if learned is not None else 5) + (1 if wl.graph else 0)),
         "learned_cull": learned,
         "state_ring": ring,
         "ball_prediction": pred,

@@ -247,6 +247,71 @@ void buildBvh(MeshBuild& m) {
 
 }  // namespace
 
+// Squared Euclidean distance (in voxels) from every voxel centre to the nearest centre of a
+// voxel with a mesh bit: three one-dimensional passes, each the lower envelope of parabolas
+// (Felzenszwalb and Huttenlocher, "Distance Transforms of Sampled Functions", 2012).
+static void edt1d(const double* f, int n, double* d, std::vector<int>& v, std::vector<double>& z) {
+    const double inf = 1e20;
+    int k = 0;
+    v[0] = 0;
+    z[0] = -inf;
+    z[1] = inf;
+    for (int q = 1; q < n; q++) {
+        double s;
+        while (true) {
+            s = ((f[q] + (double)q * q) - (f[v[k]] + (double)v[k] * v[k])) / (2.0 * (q - v[k]));
+            if (s <= z[k] && k > 0) k--;
+            else break;
+        }
+        if (s <= z[k]) {  // k == 0: the new parabola replaces the first
+            v[0] = q;
+            z[0] = -inf;
+            z[1] = inf;
+            continue;
+        }
+        k++;
+        v[k] = q;
+        z[k] = s;
+        z[k + 1] = inf;
+    }
+    k = 0;
+    for (int q = 0; q < n; q++) {
+        while (z[k + 1] < (double)q) k++;
+        const double dq = (double)(q - v[k]);
+        d[q] = dq * dq + f[v[k]];
+    }
+}
+
+static void occupiedDistance2(const std::vector<uint16_t>& occ, int X, int Y, int Z, std::vector<double>& out) {
+    const double inf = 1e20;
+    const size_t nv = (size_t)X * Y * Z;
+    out.assign(nv, inf);
+    for (size_t v = 0; v < nv; v++)
+        if (occ[v]) out[v] = 0.0;
+    const int nmax = std::max(X, std::max(Y, Z));
+    std::vector<double> f(nmax), d(nmax), z(nmax + 1);
+    std::vector<int> vv(nmax);
+    auto at = [&](int x, int y, int zz) -> double& { return out[((size_t)x * Y + y) * Z + zz]; };
+    for (int x = 0; x < X; x++)  // along z
+        for (int y = 0; y < Y; y++) {
+            for (int q = 0; q < Z; q++) f[q] = at(x, y, q);
+            edt1d(f.data(), Z, d.data(), vv, z);
+            for (int q = 0; q < Z; q++) at(x, y, q) = d[q];
+        }
+    for (int x = 0; x < X; x++)  // along y
+        for (int zz = 0; zz < Z; zz++) {
+            for (int q = 0; q < Y; q++) f[q] = at(x, q, zz);
+            edt1d(f.data(), Y, d.data(), vv, z);
+            for (int q = 0; q < Y; q++) at(x, q, zz) = d[q];
+        }
+    for (int y = 0; y < Y; y++)  // along x
+        for (int zz = 0; zz < Z; zz++) {
+            for (int q = 0; q < X; q++) f[q] = at(q, y, zz);
+            edt1d(f.data(), X, d.data(), vv, z);
+            for (int q = 0; q < X; q++) at(q, y, zz) = d[q];
+        }
+}
+
 bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
     std::vector<MeshBuild> meshes;
     for (int i = 0; i < MAX_MESHES; i++) {
@@ -527,15 +592,27 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out) {
         for (size_t v = 0; v < nv; v++) out.voxOff[v + 1] += out.voxOff[v];
         S.voxOff = out.voxOff.data();
         S.voxList = out.voxList.data();
+        // distance bound of every voxel (see ArenaStatic::occDist)
+        std::vector<double> d2;
+        occupiedDistance2(out.occ, S.occX, S.occY, S.occZ, d2);
+        out.occDist.resize(nv);
+        const float cellUu = 64.f;
+        for (size_t v = 0; v < nv; v++) {
+            const double d = (std::sqrt(d2[v]) - std::sqrt(3.0)) * cellUu;
+            out.occDist[v] = (uint16_t)std::min(65535.0, std::max(0.0, std::floor(d)));
+        }
+        S.occDist = out.occDist.data();
     }
     return true;
 }
 
 ArenaStatic deviceView(const ArenaStaticHost& h, const BvhNode* nodes, const BvhSubtree* subs,
                        const V3* triVerts, const TriEdgeInfo* triInfo, const uint32_t* bpCells,
-                       const uint16_t* occ, const uint32_t* voxOff, const uint32_t* voxList) {
+                       const uint16_t* occ, const uint32_t* voxOff, const uint32_t* voxList,
+                       const uint16_t* occDist) {
     ArenaStatic v = h.view;
     v.occ = occ;
+    v.occDist = occDist;
     v.voxOff = voxOff;
     v.voxList = voxList;
     v.nodes = nodes;

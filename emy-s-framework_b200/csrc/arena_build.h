@@ -15,6 +15,7 @@ struct ArenaStaticHost {
     std::vector<uint32_t> bpCells;
     std::vector<uint16_t> occ;
     std::vector<uint32_t> voxOff, voxList;
+    std::vector<uint16_t> occDist;
     ArenaStatic view;  // pointers into the vectors above (host addresses)
     std::string error;
 };
@@ -27,6 +28,7 @@ bool buildArenaStatic(const std::string& folder, ArenaStaticHost& out);
 // Re-points out.view at a device copy whose buffers are given.
 ArenaStatic deviceView(const ArenaStaticHost& h, const BvhNode* nodes, const BvhSubtree* subs,
                        const V3* triVerts, const TriEdgeInfo* triInfo, const uint32_t* bpCells,
-                       const uint16_t* occ, const uint32_t* voxOff, const uint32_t* voxList);
+                       const uint16_t* occ, const uint32_t* voxOff, const uint32_t* voxList,
+                       const uint16_t* occDist);
 
 }  // namespace rsb

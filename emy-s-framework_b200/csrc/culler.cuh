@@ -273,15 +273,32 @@ struct CullParams {
     float dt;
 };
 
+// The voxel distance field of the static arena data (ArenaStatic::occDist), Bullet units.
+struct VoxelBound {
+    const uint16_t* dist;
+    V3 mn;
+    float inv;
+    int X, Y, Z;
+    // lower bound (uu) on the distance from a point (uu) to every mesh; 0 off the grid
+    RSB_D float at(float x, float y, float z) const {
+        const int i = (int)floorf((x * kUuToBt - mn.x) * inv), j = (int)floorf((y * kUuToBt - mn.y) * inv),
+                  k = (int)floorf((z * kUuToBt - mn.z) * inv);
+        if (i < 0 || j < 0 || k < 0 || i >= X || j >= Y || k >= Z) return 0.f;
+        return (float)__ldg(&dist[((size_t)i * Y + j) * Z + k]);
+    }
+};
+
 // Sets bit b of cull[a] when body b (0 = ball, 1 + s = car s) of arena a cannot reach
-// any static geometry during the next `ticks` ticks.  Arenas that reverted to the exact
-// path (status bit) get no bits.
-__global__ void cullKernel(const __nv_bfloat16* __restrict__ wbf, CullParams C, const uint32_t* __restrict__ ball,
-                           const uint32_t* __restrict__ car, const uint32_t* __restrict__ arena,
-                           const int32_t* __restrict__ teamSize, int N, int ticks, uint32_t* __restrict__ cull,
-                           int statusWord, uint32_t revertBit) {
-    __shared__ float sw[CM_NPARAM];
-    loadWeights(sw, wbf);
+// any static geometry during the next `ticks` ticks, by the learned bound (the MLP's estimate
+// less the calibrated margin) or, with VOXEL, by the voxel distance field.  Arenas that
+// reverted to the exact path (status bit) get no bits.
+template <bool VOXEL>
+__global__ void cullKernel(const __nv_bfloat16* __restrict__ wbf, VoxelBound vox, CullParams C,
+                           const uint32_t* __restrict__ ball, const uint32_t* __restrict__ car,
+                           const uint32_t* __restrict__ arena, const int32_t* __restrict__ teamSize, int N, int ticks,
+                           uint32_t* __restrict__ cull, int statusWord, uint32_t revertBit) {
+    __shared__ float sw[VOXEL ? 1 : CM_NPARAM];
+    if (!VOXEL) loadWeights(sw, wbf);
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= N) return;
     uint32_t mask = 0;
@@ -304,7 +321,7 @@ __global__ void cullKernel(const __nv_bfloat16* __restrict__ wbf, CullParams C, 
             // exact distances to the floor, the ceiling and the two side-wall planes
             const float planes = fminf(fminf(z, ARENA_HEIGHT - z), fminf(x + ARENA_EXTENT_X, ARENA_EXTENT_X - x));
             if (planes < need) continue;
-            const float bound = mlpEval(sw, x, y, z) * CM_OUT - C.margin;
+            const float bound = VOXEL ? vox.at(x, y, z) : mlpEval(sw, x, y, z) * CM_OUT - C.margin;
             if (bound >= need) mask |= 1u << b;
         }
     }

@@ -352,6 +352,9 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
     }
 }
 
+// The seed counter of a captured env step: advanced once per replay.
+__global__ void advanceSeedKernel(uint64_t* seed) { *seed += 1; }
+
 // ------------------------------------------------------------------ rewards and terminals
 
 __global__ void rewardKernel(EnvView E, RewardParams R, int stepTicks) {
@@ -529,9 +532,10 @@ RSB_D M3 angleRot(float yaw, float pitch, float roll) { return m3fromEulerZYX(-r
 // Arena i of the list `idx` (every arena when idx is null; with `onlyDone`, only the
 // arenas whose terminal flag is set).
 __global__ void resetKernel(EnvView E, EnvTables Tb, ResetCurriculum Cu, const int32_t* idx, int n, uint64_t seed,
-                            int mode, bool onlyDone) {
+                            int mode, bool onlyDone, const uint64_t* seedPtr = nullptr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (seedPtr) seed = *seedPtr;  // a replayed graph reads the seed of this launch from the device
     const int a = idx ? idx[i] : i;
     if (onlyDone && E.terminals[a] == 0) return;
     const int T = E.teamSize[a], M = 2 * T, base = E.carOffset[a];

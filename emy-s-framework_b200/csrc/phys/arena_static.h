@@ -78,6 +78,10 @@ struct ArenaStatic {
     // visit them.
     const uint32_t* voxOff;
     const uint32_t* voxList;
+    // Per voxel, a lower bound (uu, rounded down) on the distance from any point of the voxel
+    // to any mesh triangle: the distance between its centre and the nearest voxel with a mesh
+    // bit, less the voxel diagonal (64 * sqrt(3) uu).
+    const uint16_t* occDist;
     V3 occMin;
     float occInvCell;
     int occX, occY, occZ;

@@ -47,6 +47,7 @@ struct DevStatic {
     uint16_t* occ = nullptr;
     uint32_t* voxOff = nullptr;
     uint32_t* voxList = nullptr;
+    uint16_t* occDist = nullptr;
     ArenaStatic view{};
 };
 
@@ -140,6 +141,10 @@ struct rsb_handle {
     size_t predCap = 0;
     size_t stageWords = 0;
     EnvTables tables{};
+    // captured env step (rsb_env_graph_capture)
+    cudaGraphExec_t envGraph = nullptr;
+    uint64_t* dGraphSeed = nullptr;
+    int graphTicks = 0;
     ResetCurriculum curriculum{{1.f, 0.f, 0.f, 0.f}, 0.f};
     bool hasRewards = false;
     RewardParams rewardParams{};
@@ -437,7 +442,7 @@ static EngineView devView(rsb_handle* h) {
     D.controls = reinterpret_cast<const CtlRec*>(h->dControls);
     D.seed = (uint32_t)(h->seed ^ (h->seed >> 32));
     D.cull = nullptr;
-    D.cullAudit = h->cullMode == RSB_CULL_LEARNED_AUDIT;
+    D.cullAudit = h->cullMode == RSB_CULL_LEARNED_AUDIT || h->cullMode == RSB_CULL_VOXEL_AUDIT;
     D.counters = h->dCounters;
     D.work = h->dWork;
     return D;
@@ -523,7 +528,7 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
     else defaultMutators(&h->mut);
     computeParams(h->mut, h->P);
     h->obsStride = RSB_OBS_BASE + RSB_OBS_PER_CAR * h->maxCars;
-    if (cfg->cull_mode < RSB_CULL_EXACT || cfg->cull_mode > RSB_CULL_LEARNED_AUDIT)
+    if (cfg->cull_mode < RSB_CULL_EXACT || cfg->cull_mode > RSB_CULL_VOXEL_AUDIT)
         return fail(nullptr, RSB_ERR_INVALID, "unknown cull mode");
     h->cullMode = cfg->cull_mode;
     h->cullSlack = cfg->cull_margin;
@@ -587,10 +592,10 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
             };
             if (!up(D->nodes, H->nodes) || !up(D->subs, H->subs) || !up(D->triVerts, H->triVerts) ||
                 !up(D->triInfo, H->triInfo) || !up(D->bpCells, H->bpCells) || !up(D->occ, H->occ) ||
-                !up(D->voxOff, H->voxOff) || !up(D->voxList, H->voxList))
+                !up(D->voxOff, H->voxOff) || !up(D->voxList, H->voxList) || !up(D->occDist, H->occDist))
                 return fail(nullptr, RSB_ERR_CUDA, "uploading arena meshes failed");
             D->view = deviceView(*H, D->nodes, D->subs, D->triVerts, D->triInfo, D->bpCells, D->occ, D->voxOff,
-                                 D->voxList);
+                                 D->voxList, D->occDist);
             // the host CPU's rsqrtss estimate, which btVector3::normalize starts from
             if (!c.rsqrtSampled) {
                 c.rsqrtExact = sampleRsqrtTable(c.rsqrtTable);
@@ -670,6 +675,8 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
     cudaFree(h->dTris);
     cudaFree(h->dObs); cudaFree(h->dObsSrc); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
+    if (h->envGraph) cudaGraphExecDestroy(h->envGraph);
+    cudaFree(h->dGraphSeed);
     cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage); cudaFree(h->dWork); cudaFree(h->dPred);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -728,10 +735,14 @@ rsb_status rsb_step(rsb_handle* h, int32_t ticks, void* stream) {
     RSB_CUDA(cudaSetDevice(h->device));
     EngineView D = devView(h);
     cudaStream_t st = pick(h, stream);
-    if (h->cullMode != RSB_CULL_EXACT && h->cullerReady) {
-        cullKernel<<<(h->N + 127) / 128, 128, 0, st>>>(h->dCwBf, h->cullParams, h->dBall, h->dCar, h->dArena,
-                                                       h->dTeamSize, h->N, ticks, h->dCull,
-                                                       (int)(offsetof(ArenaP, status) / 4), WS_CULL_MISS);
+    const bool voxel = h->cullMode == RSB_CULL_VOXEL || h->cullMode == RSB_CULL_VOXEL_AUDIT;
+    if (h->cullMode != RSB_CULL_EXACT && (h->cullerReady || voxel)) {
+        const ArenaStatic& S = h->stat->view;
+        const VoxelBound vb{S.occDist, S.occMin, S.occInvCell, S.occX, S.occY, S.occZ};
+        auto k = voxel ? cullKernel<true> : cullKernel<false>;
+        k<<<(h->N + 127) / 128, 128, 0, st>>>(h->dCwBf, vb, h->cullParams, h->dBall, h->dCar, h->dArena, h->dTeamSize,
+                                             h->N, ticks, h->dCull, (int)(offsetof(ArenaP, status) / 4),
+                                             WS_CULL_MISS);
         RSB_CUDA(cudaGetLastError());
         D.cull = h->dCull;
     }
@@ -1363,7 +1374,7 @@ rsb_status rsb_culler_gradients(rsb_handle* h, const float* pts, const float* ta
 }
 
 rsb_status rsb_set_cull_mode(rsb_handle* h, int32_t mode) {
-    if (!h || mode < RSB_CULL_EXACT || mode > RSB_CULL_LEARNED_AUDIT) return fail(h, RSB_ERR_INVALID, "unknown cull mode");
+    if (!h || mode < RSB_CULL_EXACT || mode > RSB_CULL_VOXEL_AUDIT) return fail(h, RSB_ERR_INVALID, "unknown cull mode");
     h->cullMode = mode;
     return RSB_OK;
 }
@@ -1761,6 +1772,59 @@ rsb_status rsb_reset_done(rsb_handle* h, uint64_t seed, int32_t mode, void* stre
     resetKernel<<<(h->N + 127) / 128, 128, 0, pick(h, stream)>>>(envView(h), h->tables, h->curriculum, nullptr, h->N,
                                                                   seed, mode, true);
     RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+rsb_status rsb_env_graph_capture(rsb_handle* h, const int32_t* d_actions, int32_t tick_skip, int32_t reset_mode,
+                                 uint64_t seed) {
+    if (!h || !d_actions || tick_skip <= 0) return fail(h, RSB_ERR_INVALID, "bad graph capture arguments");
+    if (reset_mode < RSB_RESET_KICKOFF || reset_mode > RSB_RESET_CURRICULUM)
+        return fail(h, RSB_ERR_INVALID, "unknown reset mode");
+    if (!h->dLut) return fail(h, RSB_ERR_STATE, "no action table uploaded");
+    if (!h->hasRewards) return fail(h, RSB_ERR_STATE, "no reward configuration at create");
+    RSB_CUDA(cudaSetDevice(h->device));
+    if (h->envGraph) {
+        cudaGraphExecDestroy(h->envGraph);
+        h->envGraph = nullptr;
+    }
+    if (!h->dGraphSeed && cudaMalloc((void**)&h->dGraphSeed, sizeof(uint64_t)) != cudaSuccess)
+        return fail(h, RSB_ERR_NOMEM, "graph seed allocation failed");
+    RSB_CUDA(cudaMemcpy(h->dGraphSeed, &seed, sizeof seed, cudaMemcpyHostToDevice));
+    const uint64_t ticksBefore = h->stats.ticks_simulated;
+    RSB_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    rsb_status st = rsb_set_actions_device(h, d_actions, h->numCars, h->stream);
+    if (st == RSB_OK) st = rsb_step(h, tick_skip, h->stream);
+    if (st == RSB_OK) st = rsb_build_obs(h, h->stream);
+    if (st == RSB_OK) st = rsb_build_rewards_terminals(h, tick_skip, h->stream);
+    if (st == RSB_OK) {
+        resetKernel<<<(h->N + 127) / 128, 128, 0, h->stream>>>(envView(h), h->tables, h->curriculum, nullptr, h->N,
+                                                               0, reset_mode, true, h->dGraphSeed);
+        advanceSeedKernel<<<1, 1, 0, h->stream>>>(h->dGraphSeed);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->stats.ticks_simulated = ticksBefore;
+    if (st != RSB_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return cudaFail(h, "cudaStreamEndCapture", e);
+    const cudaError_t ie = cudaGraphInstantiate(&h->envGraph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        h->envGraph = nullptr;
+        return cudaFail(h, "cudaGraphInstantiate", ie);
+    }
+    h->graphTicks = tick_skip;
+    return RSB_OK;
+}
+
+rsb_status rsb_env_graph_launch(rsb_handle* h, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    if (!h->envGraph) return fail(h, RSB_ERR_STATE, "no env step captured");
+    RSB_CUDA(cudaSetDevice(h->device));
+    RSB_CUDA(cudaGraphLaunch(h->envGraph, pick(h, stream)));
+    h->stats.ticks_simulated += (uint64_t)h->N * h->graphTicks;
     return RSB_OK;
 }
 

@@ -30,7 +30,7 @@ RSB_OBS_PER_CAR = 29
 RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS, RSB_BUF_BALL_PRED = range(7)
 RSB_MAX_PRED_SLICES = 8
 RSB_MAX_PRED_TICKS = 4096
-RSB_CULL_EXACT, RSB_CULL_LEARNED, RSB_CULL_LEARNED_AUDIT = 0, 1, 2
+RSB_CULL_EXACT, RSB_CULL_LEARNED, RSB_CULL_LEARNED_AUDIT, RSB_CULL_VOXEL, RSB_CULL_VOXEL_AUDIT = 0, 1, 2, 3, 4
 RSB_CULLER_PARAMS = 4481
 RSB_RESET_KICKOFF, RSB_RESET_RANDOM_STATE, RSB_RESET_HIGH_CONTACT, RSB_RESET_CURRICULUM = 0, 1, 2, 3
 RSB_MATH_RSQRT_EST, RSB_MATH_SIN, RSB_MATH_COS, RSB_MATH_ASIN, RSB_MATH_ATAN2 = range(5)
@@ -253,6 +253,8 @@ _SIGS = {
     "rsb_last_error": [_P, C.c_char_p, C.c_size_t],
     "rsb_eval_refmath": [C.c_int32, _P, _P, _P, C.c_int64, C.c_int32],
     "rsb_set_reset_curriculum": [_P, C.c_float, C.c_float, C.c_float, C.c_float],
+    "rsb_env_graph_capture": [_P, _P, C.c_int32, C.c_int32, C.c_uint64],
+    "rsb_env_graph_launch": [_P, _P],
 }
 
 #: every symbol include/rsb.h declares (checked by the ABI tests)
@@ -514,6 +516,13 @@ class Batch:
     def reset_arenas(self, idx, seed: int, mode: int = RSB_RESET_KICKOFF):
         a = np.ascontiguousarray(idx, np.int32)
         self._check(self.lib.rsb_reset_arenas(self._h, _ptr(a), len(a), seed, mode))
+
+    def env_graph_capture(self, d_actions: int, tick_skip: int, reset_mode: int, seed: int):
+        """rsb_env_graph_capture: one env step (actions from the device buffer d_actions) as a graph."""
+        self._check(self.lib.rsb_env_graph_capture(self._h, C.c_void_p(d_actions), tick_skip, reset_mode, seed))
+
+    def env_graph_launch(self, stream: int | None = None):
+        self._check(self.lib.rsb_env_graph_launch(self._h, C.c_void_p(stream or 0)))
 
     def set_reset_curriculum(self, kickoff_w: float, fuzzed_w: float, aerial_w: float, chase_w: float = 0.0):
         self._check(self.lib.rsb_set_reset_curriculum(self._h, kickoff_w, fuzzed_w, aerial_w, chase_w))

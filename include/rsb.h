@@ -92,8 +92,12 @@ enum {
     RSB_CULL_EXACT = 0,         /* every query runs the exact BVH narrowphase */
     RSB_CULL_LEARNED = 1,       /* a learned distance bound skips the static tests of bodies it
                                    places clear of every static shape for the launch */
-    RSB_CULL_LEARNED_AUDIT = 2  /* as LEARNED, but the skipped tests run anyway: whatever they find
+    RSB_CULL_LEARNED_AUDIT = 2, /* as LEARNED, but the skipped tests run anyway: whatever they find
                                    counts as a missed contact and reverts the arena to EXACT */
+    RSB_CULL_VOXEL = 3,         /* as LEARNED with a bound that is not learned: the distance from the
+                                   body's 64 uu voxel to the nearest voxel holding a mesh triangle,
+                                   less the voxel diagonal (exact lower bound, needs no training) */
+    RSB_CULL_VOXEL_AUDIT = 4    /* as VOXEL, with the skipped tests run and checked */
 };
 
 /* Reset modes for rsb_reset_arenas. */
@@ -264,6 +268,20 @@ rsb_status rsb_layout(const rsb_handle* h, int32_t* num_arenas, int32_t* num_car
 rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride);
 
 rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode);
+/* One collector env step captured as a CUDA graph (the reference launches each kernel of a
+ * step separately, RocketSimCudaApi.cuh:551-571; no counterpart there): action expansion from
+ * d_actions (device int32 [num_cars], read at every launch, so the caller refills it in
+ * place), the (culled) step of tick_skip ticks, observations + masks, rewards + terminals, and
+ * the reset of every finished arena with reset_mode.  The k-th launch resets with seed + k, so
+ * it equals the eager sequence rsb_set_actions_device, rsb_step, rsb_build_obs,
+ * rsb_build_rewards_terminals, rsb_reset_done(seed + k).  The cull mode and the step kernel's
+ * launch configuration in force at capture are the ones replayed.  Captured on the handle's
+ * stream; a new capture replaces the old one.  Needs an action table and a reward
+ * configuration. */
+rsb_status rsb_env_graph_capture(rsb_handle* h, const int32_t* d_actions, int32_t tick_skip, int32_t reset_mode,
+                                 uint64_t seed);
+/* Replays the captured env step on `stream` (NULL = the handle's stream). */
+rsb_status rsb_env_graph_launch(rsb_handle* h, void* stream);
 /* Weights of the RSB_RESET_CURRICULUM modes (RocketSimCudaBatch::SetResetCurriculum,
  * RocketSimCuda.h:283): relative weights of kickoff, fuzzed kickoff (ball and cars moved a
  * little, mild ball velocity), aerial (ball raised near midfield, one car below it) and ball

@@ -1072,6 +1072,14 @@ rsb_status rsb_set_reset_curriculum(rsb_handle* h, float, float, float, float) {
     return h ? RSB_OK : RSB_ERR_INVALID;
 }
 
+// CUDA graphs have no counterpart on the CPU oracle.
+rsb_status rsb_env_graph_capture(rsb_handle* h, const int32_t*, int32_t, int32_t, uint64_t) {
+    return fail(h, RSB_ERR_UNSUPPORTED, "no CUDA graphs on the CPU oracle");
+}
+rsb_status rsb_env_graph_launch(rsb_handle* h, void*) {
+    return fail(h, RSB_ERR_UNSUPPORTED, "no CUDA graphs on the CPU oracle");
+}
+
 rsb_status rsb_reset_arenas(rsb_handle* h, const int32_t* idx, int32_t n, uint64_t seed, int32_t mode) {
     if (!h || (n > 0 && !idx)) return RSB_ERR_INVALID;
     if (mode != RSB_RESET_KICKOFF && mode != RSB_RESET_RANDOM_STATE)

@@ -183,6 +183,21 @@ int64_t rsb_host_refmath_check(int32_t fn, uint32_t stride, uint32_t offset, int
     return nb;
 }
 
+// The voxel distance bound (ArenaStatic::occDist, uu) of the handle's static data at n points
+// (uu, 3 floats each): 0 off the grid.
+int32_t rsb_host_voxel_bound(const rsb_handle* h, const float* pts, int64_t n, float* out) {
+    if (!h || !pts || !out) return RSB_ERR_INVALID;
+    const ArenaStatic& S = h->S.view;
+    for (int64_t i = 0; i < n; i++) {
+        const int x = (int)std::floor((pts[3 * i] * kUuToBt - S.occMin.x) * S.occInvCell);
+        const int y = (int)std::floor((pts[3 * i + 1] * kUuToBt - S.occMin.y) * S.occInvCell);
+        const int z = (int)std::floor((pts[3 * i + 2] * kUuToBt - S.occMin.z) * S.occInvCell);
+        const bool in = x >= 0 && y >= 0 && z >= 0 && x < S.occX && y < S.occY && z < S.occZ;
+        out[i] = in ? (float)S.occDist[((size_t)x * S.occY + y) * S.occZ + z] : 0.f;
+    }
+    return RSB_OK;
+}
+
 rsb_status rsb_host_register(void*, size_t) { return RSB_OK; }
 rsb_status rsb_host_unregister(void*) { return RSB_OK; }
 

@@ -41,3 +41,31 @@ def test_mesh_triangles(meshes_dir):
     t = cr.load_mesh_triangles(meshes_dir)
     assert t.shape == (8020, 3, 3)
     assert np.abs(t[..., 0]).max() < 4200 and np.abs(t[..., 1]).max() < 6100
+
+
+def test_voxel_bound_is_a_lower_bound(pkg, meshes_dir):
+    """The voxel distance field behind RSB_CULL_VOXEL (built on the host from the mesh
+    occupancy grid) never exceeds the exact float64 distance to the arena meshes, and is
+    informative away from them."""
+    import ctypes as C
+
+    from host_util import build_host_engine
+
+    rsb = pkg.rsb
+    lib = rsb.load_library(build_host_engine())
+    fn = lib.rsb_host_voxel_bound
+    fn.restype = C.c_int32
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    b = rsb.Batch(lib, 1, team_size=1, meshes_path=meshes_dir, threads=1)
+    tris = cr.load_mesh_triangles(meshes_dir)
+    rng = np.random.default_rng(9)
+    n = 3000
+    pts = np.stack([rng.uniform(-4400, 4400, n), rng.uniform(-6300, 6300, n), rng.uniform(-200, 2300, n)], 1)
+    near = tris[rng.integers(0, len(tris), 1000)].mean(axis=1) + rng.normal(0, 150, (1000, 3))
+    pts = np.concatenate([pts, near]).astype(np.float32)
+    out = np.zeros(len(pts), np.float32)
+    assert fn(b._h, pts.ctypes.data, len(pts), out.ctypes.data) == 0
+    exact = cr.point_triangle_distance(pts.astype(np.float64), tris)
+    assert (out <= exact + 1e-3).all(), f"bound above the exact distance by {float((out - exact).max()):.3g} uu"
+    far = exact > 400
+    assert far.any() and np.median(out[far] / exact[far]) > 0.5

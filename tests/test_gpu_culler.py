@@ -135,3 +135,50 @@ def test_learned_step_matches_exact(pkg, meshes_dir, trained):
     assert le[2]["narrowphase_queries"] < ex[2]["narrowphase_queries"]
     assert le[0] == ex[0] and le[1] == ex[1]
     assert au[0] == ex[0] and au[1] == ex[1]
+
+
+def _culled_runs(pkg, meshes_dir, modes, w=None, margin=None, n=2048):
+    """The same seeded rollout (random-state starts, a quarter of the arenas high-contact) under
+    each cull mode: final states and the library's counters."""
+    rsb = pkg.rsb
+    runs = {}
+    for mode in modes:
+        b = _batch(pkg, meshes_dir, n=n, team_size=3, cull=mode)
+        b.set_action_lut(rsb.default_action_lut(b.lib))
+        if mode in (rsb.RSB_CULL_LEARNED, rsb.RSB_CULL_LEARNED_AUDIT):
+            b.culler_set(w, margin)
+        b.reset_all(7, rsb.RSB_RESET_RANDOM_STATE)
+        b.reset_arenas(np.arange(0, n, 4, dtype=np.int32), 8, rsb.RSB_RESET_HIGH_CONTACT)
+        rng = np.random.default_rng(5)
+        for _ in range(8):
+            b.set_actions(rng.integers(0, 90, b.num_cars).astype(np.int32))
+            b.step(8)
+        runs[mode] = (b.get_cars().tobytes(), b.get_balls().tobytes(), b.stats())
+    return runs
+
+
+def test_voxel_bound_step_matches_exact(pkg, meshes_dir):
+    """RSB_CULL_VOXEL skips the static tests of bodies its (exact) voxel distance bound clears:
+    the step equals the exact step bit for bit, and under audit the skipped tests find nothing."""
+    rsb = pkg.rsb
+    runs = _culled_runs(pkg, meshes_dir, (rsb.RSB_CULL_EXACT, rsb.RSB_CULL_VOXEL, rsb.RSB_CULL_VOXEL_AUDIT))
+    ex, vx, au = runs[rsb.RSB_CULL_EXACT], runs[rsb.RSB_CULL_VOXEL], runs[rsb.RSB_CULL_VOXEL_AUDIT]
+    assert vx[2]["culled_queries"] > 0
+    assert au[2]["missed_contacts"] == 0 and au[2]["arenas_reverted"] == 0
+    assert vx[0] == ex[0] and vx[1] == ex[1]
+    assert au[0] == ex[0] and au[1] == ex[1]
+
+
+def test_learned_bound_against_voxel_bound(pkg, meshes_dir, trained):
+    """What the trained network adds over the bound that needs no training, on one rollout:
+    the share of static tests each skips (printed).  The voxel bound is exact but coarse (64 uu
+    voxels, less their diagonal); the network's estimate is finer but gives up its calibrated
+    margin everywhere.  Both skip some tests and leave the results bit-identical."""
+    rsb = pkg.rsb
+    _, w, margin = trained
+    runs = _culled_runs(pkg, meshes_dir, (rsb.RSB_CULL_LEARNED, rsb.RSB_CULL_VOXEL), w, margin)
+    le, vx = runs[rsb.RSB_CULL_LEARNED][2], runs[rsb.RSB_CULL_VOXEL][2]
+    share = lambda s: s["culled_queries"] / max(1, s["culled_queries"] + s["narrowphase_queries"])
+    print(f"CULL learned skips {share(le):.4f} of static tests, voxel {share(vx):.4f}, margin {margin:.1f} uu")
+    assert runs[rsb.RSB_CULL_LEARNED][0] == runs[rsb.RSB_CULL_VOXEL][0]
+    assert share(le) > 0 and share(vx) > 0

@@ -62,7 +62,6 @@ struct EnvView {
     CtlRec* controls;
     float* obs;
     int stride;
-    const uint16_t* obsSrc;  // [team size 1..3][slot][column] -> offset in the arena's block row
     uint8_t* masks;
     float* rewards;
     uint8_t* terminals;
@@ -93,71 +92,41 @@ RSB_D float vdot4(float ax, float ay, float az, float bx, float by, float bz) {
 
 // ------------------------------------------------------------------ observations
 
-// Per-arena inputs staged in shared memory, one column per arena of the block.
-constexpr int OBS_ARENAS = 8;
-constexpr int OI_BALL = 0;                                   // pos, vel, ang (uu)
-constexpr int OI_CAR = 9;                                    // per car, OI_CAR_N words
-constexpr int OI_CAR_N = 20;                                 // pos vel ang fwd right up boost flags
-constexpr int OI_PREV = OI_CAR + MAX_CARS * OI_CAR_N;        // per car, 8 action values
-constexpr int OI_PAD = OI_PREV + MAX_CARS * 8;               // 2 frames x 34 pad values
-constexpr int OI_MASK = OI_PAD + 2 * NUM_PADS;               // per car, 3 mask words
-constexpr int OI_TEAM = OI_MASK + MAX_CARS * 3;              // team size
-constexpr int OI_WORDS = OI_TEAM + 1;
-// flag bits of the staged car
-constexpr uint32_t OF_GROUND = 1, OF_FLIPJUMP = 2, OF_DEMOED = 4, OF_JUMPED = 8, OF_ORANGE = 16;
+// A row of AdvancedObs (AdvancedObs.cpp:25-65) for player p of an arena of team size T, in
+// the frame of p's team (orange = InvertPhys): ball (9), p's action (8), pad values (34),
+// then 2T car blocks of 29 (p, its teammates by descending slot, the opponents by descending
+// slot), then zeros up to the batch's row stride.
+constexpr int OBS_STRIDE_MAX = RSB_OBS_BASE + RSB_OBS_PER_CAR * MAX_CARS;
+constexpr int OBS_COL_PREV = 9, OBS_COL_PAD = 17, OBS_COL_CAR = RSB_OBS_BASE;
 
-// The parts of a row that do not depend on the viewing player itself, built once per arena:
-// the ball block and every car's 29-value block, in each team's frame (orange = InvertPhys).
-// A row is a gather from the arena's block row: ball (per frame), pad values (per frame), the
-// cars' actions, the car blocks, and a zero for the padding of smaller arenas.
-constexpr int OB_BALL = 0;                      // [frame][9]
-constexpr int OB_PAD = OB_BALL + 2 * 9;         // [frame][34]
-constexpr int OB_PREV = OB_PAD + 2 * NUM_PADS;  // [car][8]
-constexpr int OB_CAR = OB_PREV + MAX_CARS * 8;  // [frame][car][29]
-constexpr int OB_ZERO = OB_CAR + 2 * MAX_CARS * 29;
-constexpr int OB_WORDS = OB_ZERO + 1;           // odd row stride: fewer bank conflicts
-
-// Offset in the block row of column `col` of the observation row of slot p in an arena of
-// team size T (AdvancedObs.cpp:25-65 with the teammate / opponent order described above):
-// built once on the host for the batch's row stride.
-inline int obsSource(int T, int p, int col) {
-    if (p >= 2 * T) return OB_ZERO;
+// Index of car q's block in the row of viewer p (q, p of one arena of team size T): the
+// inverse of the order above.
+RSB_HD int obsCarIndex(int T, int p, int q) {
     const bool orange = p >= T;
-    if (col < 9) return OB_BALL + (orange ? 9 : 0) + col;
-    if (col < 17) return OB_PREV + p * 8 + (col - 9);
-    if (col < 51) return OB_PAD + (orange ? NUM_PADS : 0) + (col - 17);
-    const int k = (col - 51) / 29, j = (col - 51) - 29 * k;
-    if (k >= 2 * T) return OB_ZERO;
-    int q;
     const int ownFirst = orange ? T : 0, oppFirst = orange ? 0 : T;
-    if (k == 0) {
-        q = p;
-    } else if (k < T) {
-        // teammates, descending slot order, skipping the player
-        q = ownFirst + T - 1 - (k - 1);
-        if (q <= p) q--;
-    } else {
-        q = oppFirst + T - 1 - (k - T);
-    }
-    return OB_CAR + ((orange ? MAX_CARS : 0) + q) * 29 + j;
+    if (q == p) return 0;
+    if (q >= ownFirst && q < ownFirst + T) return 1 + (ownFirst + T - 1 - q) - (p > q ? 1 : 0);
+    return T + (oppFirst + T - 1 - q);
 }
-inline void obsSourceTable(int stride, uint16_t* tab) {
-    for (int T = 1; T <= RSB_MAX_TEAM_SIZE; T++)
-        for (int p = 0; p < MAX_CARS; p++)
-            for (int col = 0; col < stride; col++)
-                tab[((T - 1) * MAX_CARS + p) * stride + col] = (uint16_t)obsSource(T, p, col);
-}
+
+// Per-arena inputs of the car blocks, staged in shared memory, one column per arena.
+constexpr int OBS_ARENAS = 4;
+constexpr int OI_BALL = 0;                        // ball pos, vel (uu)
+constexpr int OI_CAR = 6;                         // per car, OI_CAR_N words
+constexpr int OI_CAR_N = 21;                      // pos vel ang fwd right up boost flags, 1 pad word
+                                                  // (an odd stride keeps the cars on distinct banks)
+constexpr int OI_MASK = OI_CAR + MAX_CARS * OI_CAR_N;  // per car, 3 mask words
+constexpr int OI_WORDS = OI_MASK + MAX_CARS * 3;
+// flag bits of the staged car
+constexpr uint32_t OF_GROUND = 1, OF_FLIPJUMP = 2, OF_DEMOED = 4, OF_JUMPED = 8;
 
 struct ObsShared {
+    // the block's rows, flat, at the same offset modulo 16 bytes as in the output buffer
+    __align__(16) float stage[OBS_ARENAS * MAX_CARS * OBS_STRIDE_MAX + 4];
     float in[OI_WORDS][OBS_ARENAS];
-    union {
-        float blk[OBS_ARENAS][OB_WORDS];
-        struct {                                 // staging of the pad records (phase A only)
-            float cool[NUM_PADS][OBS_ARENAS];
-            uint32_t act[NUM_PADS][OBS_ARENAS];
-        } pad;
-    };
-    uint16_t rowOf[OBS_ARENAS * MAX_CARS];   // local row -> arena (low byte) | slot << 8
+    uint8_t rowBase[OBS_ARENAS];              // first row of each arena, in the block
+    uint8_t team[OBS_ARENAS];
+    uint8_t rowOf[OBS_ARENAS * MAX_CARS];     // block row -> arena | slot << 4
 };
 
 // The 29 values of car q's block in one frame (inv: the orange frame, InvertPhys), written to
@@ -197,13 +166,24 @@ RSB_D void obsCarBlock(const ObsShared& S, int la, int q, bool inv, float* o) {
     o[28] = (f & OF_JUMPED) ? 1.f : 0.f;
 }
 
-// A block serves 8 arenas (24 KB of shared memory, so that 9 blocks share an SM and overlap
-// their phases) in three phases, every thread taking part in each:
-//   A. stage the arenas' records from the word planes (consecutive threads read consecutive
-//      arenas of one word: coalesced), derive flags, masks, pad values and the actions;
-//   B. build the ball block and the 29-value block of every car once per team frame;
-//   C. write the arenas' rows, which are contiguous in the output, as 16-byte stores of four
-//      elements assembled from the blocks, and the mask bytes as 32-bit words.
+// Four mask bits from bit b of a 96-bit action mask, spread to four bytes of 0 / 1 (byte t of
+// the little-endian word = bit b + t).
+RSB_D uint32_t maskNibbleBytes(uint32_t m0, uint32_t m1, uint32_t m2, int b) {
+    const int w = b >> 5;
+    const uint32_t lo = w == 0 ? m0 : (w == 1 ? m1 : m2), hi = w == 0 ? m1 : (w == 1 ? m2 : 0u);
+    const uint32_t x = __funnelshift_r(lo, hi, b & 31) & 15u;
+    return (x * 0x00204081u) & 0x01010101u;
+}
+
+// A block serves 4 arenas (24 KB of shared memory: 9 blocks share an SM) in three phases,
+// every thread taking part in each:
+//   A. read the arenas' word planes (consecutive threads on consecutive arenas of one word),
+//      stage what the car blocks need, and write the ball, action and pad columns of every
+//      row straight into the staged rows;
+//   B. write every car's 29-value block, once per team frame, into the rows of that frame's
+//      viewers, and the mask bytes of the block's rows to the output as 32-bit words;
+//   C. send the staged rows out: the 16-byte-aligned middle as one bulk copy from shared
+//      memory (cp.async.bulk), the few elements either side as plain stores.
 constexpr int OBS_THREADS = 128;
 __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb) {
     __shared__ ObsShared S;
@@ -212,144 +192,169 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
     if (a0 >= E.N) return;
     const int na = min(OBS_ARENAS, E.N - a0);
     const int row0 = E.carOffset[a0];
-
-    // ---- A: ball words and team sizes
-    for (int i = tid; i < 10 * OBS_ARENAS; i += OBS_THREADS) {
-        const int la = i % OBS_ARENAS, w = i / OBS_ARENAS, a = a0 + la;
-        if (la >= na) continue;
-        if (w == 9) {
-            S.in[OI_TEAM][la] = (float)E.teamSize[a];
-        } else {
-            const int k = w % 3;
-            const float v = w < 3 ? ballF(E, a, BW_POS + k) * kBtToUu
-                                  : (w < 6 ? ballF(E, a, BW_LIN + k) * kBtToUu : ballF(E, a, BW_ANG + k));
-            S.in[OI_BALL + w][la] = v;
-        }
-    }
-    // cars: one (arena, slot) per thread
-    for (int i = tid; i < MAX_CARS * OBS_ARENAS; i += OBS_THREADS) {
-        const int la = i % OBS_ARENAS, s = i / OBS_ARENAS, a = a0 + la;
-        if (la >= na || s >= 2 * E.teamSize[a]) continue;
-        const int o = OI_CAR + s * OI_CAR_N;
-        for (int k = 0; k < 3; k++) {
-            S.in[o + k][la] = carF(E, a, s, CW_POS + k) * kBtToUu;
-            S.in[o + 3 + k][la] = carF(E, a, s, CW_LIN + k) * kBtToUu;
-            S.in[o + 6 + k][la] = carF(E, a, s, CW_ANG + k);
-            // CarState::rotMat columns: forward, right, up (basis rows stored)
-            S.in[o + 9 + k][la] = carF(E, a, s, CW_ROTMAT + 3 * k + 0);
-            S.in[o + 12 + k][la] = carF(E, a, s, CW_ROTMAT + 3 * k + 1);
-            S.in[o + 15 + k][la] = carF(E, a, s, CW_ROTMAT + 3 * k + 2);
-        }
-        const float boost = carF(E, a, s, CW_BOOST);
-        S.in[o + 18][la] = boost;
-        const uint32_t cf = carW(E, a, s, CW_FLAGS);
-        const bool ground = cf & CF_ON_GROUND;
-        // CarState::HasFlipOrJump (Car.cpp:285-289)
-        const bool flipJump = ground || (!(cf & CF_HAS_FLIPPED) && !(cf & CF_HAS_DOUBLE_JUMPED) &&
-                                         carF(E, a, s, CW_AIRSJ) < DOUBLEJUMP_MAX_DELAY);
-        const uint32_t of = (ground ? OF_GROUND : 0u) | (flipJump ? OF_FLIPJUMP : 0u) |
-                            ((cf & CF_DEMOED) ? OF_DEMOED : 0u) | ((cf & CF_HAS_JUMPED) ? OF_JUMPED : 0u) |
-                            ((cf & CF_TEAM_ORANGE) ? OF_ORANGE : 0u);
-        S.in[o + 19][la] = __uint_as_float(of);
-        // DefaultAction::GetActionMask
-        const bool turtled = (cf & CF_WORLD_CONTACT) && carF(E, a, s, CW_WCN + 2) > 0.9f;
-        for (int w = 0; w < 3; w++) {
-            uint32_t m = ground ? Tb.ground[w] : Tb.air[w];
-            if (boost == 0.f) m &= ~Tb.boost[w];
-            if (flipJump || turtled) m |= Tb.jump[w];
-            S.in[OI_MASK + s * 3 + w][la] = __uint_as_float(m);
-        }
-        // the step's action (EnvSet passes the parsed Action as prevAction)
-        const int base = E.carOffset[a];
-        const CtlRec c = E.controls[base + s];
-        for (int k = 0; k < 5; k++) S.in[OI_PREV + s * 8 + k][la] = c.v[k];
-        S.in[OI_PREV + s * 8 + 5][la] = c.jump ? 1.f : 0.f;
-        S.in[OI_PREV + s * 8 + 6][la] = c.boost ? 1.f : 0.f;
-        S.in[OI_PREV + s * 8 + 7][la] = c.handbrake ? 1.f : 0.f;
-        S.rowOf[base - row0 + s] = (uint16_t)(la | (s << 8));
-    }
-    // pad records
-    for (int i = tid; i < NUM_PADS * OBS_ARENAS; i += OBS_THREADS) {
-        const int la = i % OBS_ARENAS, p = i / OBS_ARENAS, a = a0 + la;
-        if (la >= na) continue;
-        S.pad.cool[p][la] = __uint_as_float(E.pad[((size_t)0 * NUM_PADS + p) * E.N + a]);
-        S.pad.act[p][la] = E.pad[((size_t)1 * NUM_PADS + p) * E.N + a] & 1u;
-    }
-    __syncthreads();
-    // boost pads in RLGymCPP order; GameState::GetBoostPadTimers returns the mirrored timers for
-    // the blue frame and the direct ones for the orange frame (GameState.h:56-62), and
-    // AdvancedObs pairs them with the frame's pads
-    for (int i = tid; i < NUM_PADS * OBS_ARENAS; i += OBS_THREADS) {
-        const int la = i % OBS_ARENAS, pi = i / OBS_ARENAS;
-        if (la >= na) continue;
-        const int d = Tb.padMap[pi], m = Tb.padMap[NUM_PADS - 1 - pi];
-        S.in[OI_PAD + pi][la] = S.pad.act[d][la] ? 1.f : 1.f / (1.f + S.pad.cool[m][la]);
-        S.in[OI_PAD + NUM_PADS + pi][la] = S.pad.act[m][la] ? 1.f : 1.f / (1.f + S.pad.cool[d][la]);
-    }
-    __syncthreads();
-
-    // ---- B: the block row of every arena: ball, pad values and actions copied per frame,
-    // then one thread per (arena, car) writes that car's 29-value block in both frames
-    for (int i = tid; i < OB_CAR * OBS_ARENAS; i += OBS_THREADS) {
-        const int la = i % OBS_ARENAS, w = i / OBS_ARENAS;
-        if (la >= na) continue;
-        float v;
-        if (w < OB_PAD) {
-            const int col = w % 9;
-            v = S.in[OI_BALL + col][la] * (col < 3 ? OBS_POS : (col < 6 ? OBS_VEL : OBS_ANG));
-            if (w >= 9 && (col % 3) < 2) v = -v;
-        } else if (w < OB_PREV) {
-            v = S.in[OI_PAD + (w - OB_PAD)][la];
-        } else {
-            v = S.in[OI_PREV + (w - OB_PREV)][la];
-        }
-        S.blk[la][w] = v;
-    }
-    for (int i = tid; i < MAX_CARS * OBS_ARENAS; i += OBS_THREADS) {
-        const int la = i % OBS_ARENAS, q = i / OBS_ARENAS;
-        if (la >= na) continue;
-        S.blk[la][OB_ZERO] = 0.f;
-        const bool live = q < 2 * (int)S.in[OI_TEAM][la];
-        for (int f = 0; f < 2; f++) {
-            float* o = &S.blk[la][OB_CAR + (f * MAX_CARS + q) * 29];
-            if (live) obsCarBlock(S, la, q, f == 1, o);
-            else
-                for (int j = 0; j < 29; j++) o[j] = 0.f;
-        }
-    }
-    __syncthreads();
-
-    // ---- C: the rows (contiguous for the block's arenas), then the masks.  Each warp writes
-    // one contiguous stretch, its lanes on consecutive elements: a coalesced 128-byte store
-    // per warp instruction, and consecutive shared-memory words for consecutive lanes.
     const int rows = E.carOffset[a0 + na] - row0;
     const int stride = E.stride;
     float* out = E.obs + (size_t)row0 * stride;
-    {
-        // one warp per row, its lanes on consecutive columns
-        const int lane = tid & 31;
-        for (int r = tid >> 5; r < rows; r += OBS_THREADS / 32) {
-            const uint16_t ro = S.rowOf[r];
-            const int la = ro & 0xff, p = ro >> 8;
-            const float* blk = S.blk[la];
-            const uint16_t* src = E.obsSrc + (((int)S.in[OI_TEAM][la] - 1) * MAX_CARS + p) * stride;
-            float* o = out + (size_t)r * stride;
-            for (int col = lane; col < stride; col += 32) o[col] = blk[__ldg(src + col)];
+    const int mis = (int)((reinterpret_cast<uintptr_t>(out) >> 2) & 3);
+    float* st = S.stage + mis;
+
+    // ---- A
+    constexpr int nCar = 2 * MAX_CARS * OBS_ARENAS, nBall = 9 * OBS_ARENAS, nPad = NUM_PADS * OBS_ARENAS;
+    for (int i = tid; i < nCar + nBall + nPad; i += OBS_THREADS) {
+        if (i < nCar) {
+            // (arena, slot, half): half 0 the kinematics, half 1 flags, masks and the action
+            const int la = i % OBS_ARENAS, s = (i / OBS_ARENAS) % MAX_CARS, half = i / (OBS_ARENAS * MAX_CARS);
+            const int a = a0 + la;
+            if (la >= na) continue;
+            // every slot's words are in the planes: read them before the team size arrives
+            const int o = OI_CAR + s * OI_CAR_N;
+            if (half == 0) {
+                float v[18];
+                for (int k = 0; k < 3; k++) {
+                    v[k] = carF(E, a, s, CW_POS + k) * kBtToUu;
+                    v[3 + k] = carF(E, a, s, CW_LIN + k) * kBtToUu;
+                    v[6 + k] = carF(E, a, s, CW_ANG + k);
+                    // CarState::rotMat columns: forward, right, up (basis rows stored)
+                    v[9 + k] = carF(E, a, s, CW_ROTMAT + 3 * k + 0);
+                    v[12 + k] = carF(E, a, s, CW_ROTMAT + 3 * k + 1);
+                    v[15 + k] = carF(E, a, s, CW_ROTMAT + 3 * k + 2);
+                }
+                for (int k = 0; k < 18; k++) S.in[o + k][la] = v[k];
+                continue;
+            }
+            const int T = E.teamSize[a], base = E.carOffset[a];
+            const float boost = carF(E, a, s, CW_BOOST), airSinceJump = carF(E, a, s, CW_AIRSJ);
+            const float wcnZ = carF(E, a, s, CW_WCN + 2);
+            const uint32_t cf = carW(E, a, s, CW_FLAGS);
+            if (s >= 2 * T) continue;
+            const int rb = base - row0;
+            if (s == 0) {
+                S.rowBase[la] = (uint8_t)rb;
+                S.team[la] = (uint8_t)T;
+            }
+            S.rowOf[rb + s] = (uint8_t)(la | (s << 4));
+            S.in[o + 18][la] = boost;
+            const bool ground = cf & CF_ON_GROUND;
+            // CarState::HasFlipOrJump (Car.cpp:285-289)
+            const bool flipJump = ground || (!(cf & CF_HAS_FLIPPED) && !(cf & CF_HAS_DOUBLE_JUMPED) &&
+                                             airSinceJump < DOUBLEJUMP_MAX_DELAY);
+            const uint32_t of = (ground ? OF_GROUND : 0u) | (flipJump ? OF_FLIPJUMP : 0u) |
+                                ((cf & CF_DEMOED) ? OF_DEMOED : 0u) | ((cf & CF_HAS_JUMPED) ? OF_JUMPED : 0u);
+            S.in[o + 19][la] = __uint_as_float(of);
+            // DefaultAction::GetActionMask
+            const bool turtled = (cf & CF_WORLD_CONTACT) && wcnZ > 0.9f;
+            for (int w = 0; w < 3; w++) {
+                uint32_t m = ground ? Tb.ground[w] : Tb.air[w];
+                if (boost == 0.f) m &= ~Tb.boost[w];
+                if (flipJump || turtled) m |= Tb.jump[w];
+                S.in[OI_MASK + s * 3 + w][la] = __uint_as_float(m);
+            }
+            // the step's action (EnvSet passes the parsed Action as prevAction)
+            const CtlRec c = E.controls[base + s];
+            float* r = st + (rb + s) * stride + OBS_COL_PREV;
+            for (int k = 0; k < 5; k++) r[k] = c.v[k];
+            r[5] = c.jump ? 1.f : 0.f;
+            r[6] = c.boost ? 1.f : 0.f;
+            r[7] = c.handbrake ? 1.f : 0.f;
+        } else if (i < nCar + nBall) {
+            // ball word w in both frames, into the first 9 columns of every row
+            const int j = i - nCar, la = j % OBS_ARENAS, w = j / OBS_ARENAS, a = a0 + la;
+            if (la >= na) continue;
+            const int k = w % 3;
+            const float v = w < 3 ? ballF(E, a, BW_POS + k) * kBtToUu
+                                  : (w < 6 ? ballF(E, a, BW_LIN + k) * kBtToUu : ballF(E, a, BW_ANG + k));
+            if (w < 6) S.in[OI_BALL + w][la] = v;
+            const float blue = v * (w < 3 ? OBS_POS : (w < 6 ? OBS_VEL : OBS_ANG));
+            const float orange = k < 2 ? -blue : blue;
+            const int T = E.teamSize[a];
+            float* r = st + (E.carOffset[a] - row0) * stride + w;
+            for (int p = 0; p < 2 * T; p++) r[p * stride] = p < T ? blue : orange;
+        } else {
+            // boost pads in RLGymCPP order; GameState::GetBoostPadTimers returns the mirrored
+            // timers for the blue frame and the direct ones for the orange frame
+            // (GameState.h:56-62), and AdvancedObs pairs them with the frame's pads
+            const int j = i - nCar - nBall, la = j % OBS_ARENAS, pi = j / OBS_ARENAS, a = a0 + la;
+            if (la >= na) continue;
+            const int d = Tb.padMap[pi], m = Tb.padMap[NUM_PADS - 1 - pi];
+            const float coolD = __uint_as_float(E.pad[(size_t)d * E.N + a]);
+            const float coolM = __uint_as_float(E.pad[(size_t)m * E.N + a]);
+            const bool actD = E.pad[((size_t)NUM_PADS + d) * E.N + a] & 1u;
+            const bool actM = E.pad[((size_t)NUM_PADS + m) * E.N + a] & 1u;
+            const float blue = actD ? 1.f : 1.f / (1.f + coolM);
+            const float orange = actM ? 1.f : 1.f / (1.f + coolD);
+            const int T = E.teamSize[a];
+            float* r = st + (E.carOffset[a] - row0) * stride + OBS_COL_PAD + pi;
+            for (int p = 0; p < 2 * T; p++) r[p * stride] = p < T ? blue : orange;
         }
     }
-    // masks: rows * 90 bytes, 4-byte aligned (every arena has an even number of cars)
+    __syncthreads();
+
+    // ---- B
+    int tmin = RSB_MAX_TEAM_SIZE;
+    for (int la = 0; la < na; la++) tmin = min(tmin, (int)S.team[la]);
+    const int zcols = stride - (OBS_COL_CAR + 2 * RSB_OBS_PER_CAR * tmin);  // padding of the smallest arenas
+    const int nMask = rows / 2 * 45;  // a pair of rows is 180 mask bytes: 45 words
+    const int nZero = zcols > 0 ? rows * zcols : 0;
     uint32_t* mout = reinterpret_cast<uint32_t*>(E.masks + (size_t)row0 * RSB_NUM_ACTIONS);
-    const int nw = rows * RSB_NUM_ACTIONS / 4;
-    for (int w = tid; w < nw; w += OBS_THREADS) {
-        uint32_t word = 0;
-        for (int t = 0; t < 4; t++) {
-            const int e = 4 * w + t, r = e / RSB_NUM_ACTIONS, i = e - r * RSB_NUM_ACTIONS;
-            const uint16_t ro = S.rowOf[r];
-            const uint32_t m = __float_as_uint(S.in[OI_MASK + (ro >> 8) * 3 + (i >> 5)][ro & 0xff]);
-            word |= ((m >> (i & 31)) & 1u) << (8 * t);
+    for (int i = tid; i < nCar + nMask + nZero; i += OBS_THREADS) {
+        if (i < nCar) {
+            // car q's block in frame f, into the rows of that frame's T viewers
+            const int la = i % OBS_ARENAS, q = (i / OBS_ARENAS) % MAX_CARS, f = i / (OBS_ARENAS * MAX_CARS);
+            if (la >= na) continue;
+            const int T = S.team[la];
+            if (q >= 2 * T) continue;
+            float* row = st + S.rowBase[la] * stride + OBS_COL_CAR;
+            const int p0 = f * T;
+            float* o = row + p0 * stride + RSB_OBS_PER_CAR * obsCarIndex(T, p0, q);
+            obsCarBlock(S, la, q, f == 1, o);
+            for (int p = p0 + 1; p < p0 + T; p++) {
+                float* d = row + p * stride + RSB_OBS_PER_CAR * obsCarIndex(T, p, q);
+                for (int k = 0; k < RSB_OBS_PER_CAR; k++) d[k] = o[k];
+            }
+        } else if (i < nCar + nMask) {
+            // mask word w of row pair k (rows 2k, 2k+1: one arena, slots s, s + 1)
+            const int j = i - nCar, k = j / 45, w = j - 45 * k;
+            const int ro = S.rowOf[2 * k], la = ro & 15, s = ro >> 4;
+            const int sm = OI_MASK + s * 3;
+            uint32_t word;
+            if (w < 22) {
+                word = maskNibbleBytes(__float_as_uint(S.in[sm][la]), __float_as_uint(S.in[sm + 1][la]),
+                                       __float_as_uint(S.in[sm + 2][la]), 4 * w);
+            } else if (w > 22) {
+                word = maskNibbleBytes(__float_as_uint(S.in[sm + 3][la]), __float_as_uint(S.in[sm + 4][la]),
+                                       __float_as_uint(S.in[sm + 5][la]), 4 * (w - 23) + 2);
+            } else {
+                // bytes 88, 89 of the first row, 0, 1 of the second
+                const uint32_t x = ((__float_as_uint(S.in[sm + 2][la]) >> 24) & 3u) |
+                                   ((__float_as_uint(S.in[sm + 3][la]) & 3u) << 2);
+                word = (x * 0x00204081u) & 0x01010101u;
+            }
+            mout[j] = word;
+        } else {
+            // zero columns after the last car block of arenas smaller than the largest
+            const int j = i - nCar - nMask, r = j / zcols, c = stride - zcols + (j - r * zcols);
+            const int la = S.rowOf[r] & 15;
+            if (c >= OBS_COL_CAR + 2 * RSB_OBS_PER_CAR * S.team[la]) st[r * stride + c] = 0.f;
         }
-        mout[w] = word;
     }
+    // the staged rows are read by the bulk copy (async proxy) next
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+
+    // ---- C
+    const int total = rows * stride;
+    const int e0 = min(total, (4 - mis) & 3);
+    const int e1 = e0 + ((total - e0) & ~3);
+    if (tid == 0 && e1 > e0) {
+        const uint32_t src = (uint32_t)__cvta_generic_to_shared(st + e0);
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                     :: "l"(out + e0), "r"(src), "r"((e1 - e0) * 4) : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+    if (tid < e0) out[tid] = st[tid];
+    else if (tid >= 4 && tid - 4 < total - e1) out[e1 + tid - 4] = st[e1 + tid - 4];
+    // the shared memory must outlive the copy's reads of it; the writes complete with the grid
+    if (tid == 0 && e1 > e0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 // The seed counter of a captured env step: advanced once per replay.

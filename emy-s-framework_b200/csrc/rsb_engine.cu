@@ -110,7 +110,6 @@ struct rsb_handle {
     int32_t* dActions = nullptr;
     // env layer
     int obsStride = 0;
-    uint16_t* dObsSrc = nullptr;           // obsSourceTable of obsStride
     float* dObs = nullptr;
     uint8_t* dMasks = nullptr;
     float* dRewards = nullptr;
@@ -460,7 +459,6 @@ static EnvView envView(rsb_handle* h) {
     E.controls = reinterpret_cast<CtlRec*>(h->dControls);
     E.obs = h->dObs;
     E.stride = h->obsStride;
-    E.obsSrc = h->dObsSrc;
     E.masks = h->dMasks;
     E.rewards = h->dRewards;
     E.terminals = h->dTerminals;
@@ -639,17 +637,11 @@ rsb_status rsb_create(const rsb_config* cfg, rsb_handle** out) {
         !dalloc(h->dControls, std::max<size_t>(1, h->numCars) * sizeof(rsb_controls)) ||
         !dalloc(h->dActions, std::max<size_t>(1, h->numCars) * 4) ||
         !dalloc(h->dObs, (size_t)h->numCars * h->obsStride * 4) ||
-        !dalloc(h->dObsSrc, (size_t)RSB_MAX_TEAM_SIZE * MAX_CARS * h->obsStride * 2) ||
         !dalloc(h->dMasks, (size_t)h->numCars * RSB_NUM_ACTIONS) ||
         !dalloc(h->dRewards, (size_t)h->numCars * 4) || !dalloc(h->dTerminals, N) ||
         !dalloc(h->dResetIdx, N * 4) || !dalloc(h->dCull, N * 4) ||
         !dalloc(h->dCounters, 4 * sizeof(unsigned long long)) || !dalloc(h->dWork, sizeof(unsigned int)))
         return fail(nullptr, RSB_ERR_NOMEM, "device allocation failed");
-    {
-        std::vector<uint16_t> src((size_t)RSB_MAX_TEAM_SIZE * MAX_CARS * h->obsStride);
-        obsSourceTable(h->obsStride, src.data());
-        cudaMemcpy(h->dObsSrc, src.data(), src.size() * 2, cudaMemcpyHostToDevice);
-    }
     cudaMemcpy(h->dTeamSize, h->teamSize.data(), N * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(h->dCarOffset, h->carOffset.data(), (N + 1) * 4, cudaMemcpyHostToDevice);
     {
@@ -674,7 +666,7 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dScratch);
     cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
     cudaFree(h->dTris);
-    cudaFree(h->dObs); cudaFree(h->dObsSrc); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
+    cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
     if (h->envGraph) cudaGraphExecDestroy(h->envGraph);
     cudaFree(h->dGraphSeed);
     cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage); cudaFree(h->dWork); cudaFree(h->dPred);

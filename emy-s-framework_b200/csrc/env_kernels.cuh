@@ -175,16 +175,17 @@ RSB_D uint32_t maskNibbleBytes(uint32_t m0, uint32_t m1, uint32_t m2, int b) {
     return (x * 0x00204081u) & 0x01010101u;
 }
 
-// A block serves 4 arenas (24 KB of shared memory: 9 blocks share an SM) in three phases,
-// every thread taking part in each:
+// A block of 256 threads serves 4 arenas (24 KB of shared memory) in three phases, every
+// thread taking part in each, one item per thread where the items allow (so that a thread's
+// reads are issued together, not behind one another):
 //   A. read the arenas' word planes (consecutive threads on consecutive arenas of one word),
 //      stage what the car blocks need, and write the ball, action and pad columns of every
 //      row straight into the staged rows;
-//   B. write every car's 29-value block, once per team frame, into the rows of that frame's
-//      viewers, and the mask bytes of the block's rows to the output as 32-bit words;
+//   B. write every car's 29-value block, per team frame and viewer, into that viewer's row,
+//      and the mask bytes of the block's rows to the output as 32-bit words;
 //   C. send the staged rows out: the 16-byte-aligned middle as one bulk copy from shared
 //      memory (cp.async.bulk), the few elements either side as plain stores.
-constexpr int OBS_THREADS = 128;
+constexpr int OBS_THREADS = 256;
 __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb) {
     __shared__ ObsShared S;
     const int tid = threadIdx.x;
@@ -296,24 +297,21 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
     const int nMask = rows / 2 * 45;  // a pair of rows is 180 mask bytes: 45 words
     const int nZero = zcols > 0 ? rows * zcols : 0;
     uint32_t* mout = reinterpret_cast<uint32_t*>(E.masks + (size_t)row0 * RSB_NUM_ACTIONS);
-    for (int i = tid; i < nCar + nMask + nZero; i += OBS_THREADS) {
-        if (i < nCar) {
-            // car q's block in frame f, into the rows of that frame's T viewers
-            const int la = i % OBS_ARENAS, q = (i / OBS_ARENAS) % MAX_CARS, f = i / (OBS_ARENAS * MAX_CARS);
+    constexpr int nView = 2 * OBS_ARENAS * MAX_CARS * RSB_MAX_TEAM_SIZE;  // (arena, car, frame, viewer)
+    for (int i = tid; i < nView + nMask + nZero; i += OBS_THREADS) {
+        if (i < nView) {
+            // car q's block in frame f, into the row of viewer v of that frame's team
+            const int la = i % OBS_ARENAS, q = (i / OBS_ARENAS) % MAX_CARS, f = (i / (OBS_ARENAS * MAX_CARS)) & 1,
+                      v = i / (2 * OBS_ARENAS * MAX_CARS);
             if (la >= na) continue;
             const int T = S.team[la];
-            if (q >= 2 * T) continue;
-            float* row = st + S.rowBase[la] * stride + OBS_COL_CAR;
-            const int p0 = f * T;
-            float* o = row + p0 * stride + RSB_OBS_PER_CAR * obsCarIndex(T, p0, q);
-            obsCarBlock(S, la, q, f == 1, o);
-            for (int p = p0 + 1; p < p0 + T; p++) {
-                float* d = row + p * stride + RSB_OBS_PER_CAR * obsCarIndex(T, p, q);
-                for (int k = 0; k < RSB_OBS_PER_CAR; k++) d[k] = o[k];
-            }
-        } else if (i < nCar + nMask) {
+            if (q >= 2 * T || v >= T) continue;
+            const int p = f * T + v;
+            obsCarBlock(S, la, q, f == 1,
+                        st + (S.rowBase[la] + p) * stride + OBS_COL_CAR + RSB_OBS_PER_CAR * obsCarIndex(T, p, q));
+        } else if (i < nView + nMask) {
             // mask word w of row pair k (rows 2k, 2k+1: one arena, slots s, s + 1)
-            const int j = i - nCar, k = j / 45, w = j - 45 * k;
+            const int j = i - nView, k = j / 45, w = j - 45 * k;
             const int ro = S.rowOf[2 * k], la = ro & 15, s = ro >> 4;
             const int sm = OI_MASK + s * 3;
             uint32_t word;
@@ -332,7 +330,7 @@ __global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb
             mout[j] = word;
         } else {
             // zero columns after the last car block of arenas smaller than the largest
-            const int j = i - nCar - nMask, r = j / zcols, c = stride - zcols + (j - r * zcols);
+            const int j = i - nView - nMask, r = j / zcols, c = stride - zcols + (j - r * zcols);
             const int la = S.rowOf[r] & 15;
             if (c >= OBS_COL_CAR + 2 * RSB_OBS_PER_CAR * S.team[la]) st[r * stride + c] = 0.f;
         }

@@ -306,7 +306,7 @@ def run_ours(args, rank, world, dist):
     tune = batch.autotune(wl.tick_skip) if not args.no_autotune else []
     extra = {}
     steps = args.steps
-    if wl.preset == "c4":
+    if wl.preset == "c4" and not getattr(args, "summary", False):
         steps = max(steps, 4096 // wl.tick_skip)  # one 4096-tick rollout
     start(rsb.RSB_CULL_EXACT)
     warm()
@@ -336,42 +336,47 @@ def run_ours(args, rank, world, dist):
         start(rsb.RSB_CULL_LEARNED)
         warm()
         value, total_ms, step_times, queries = timed(steps, clocks)
-        # the same run once more with the skipped tests executed and checked
-        start(rsb.RSB_CULL_LEARNED_AUDIT)
-        s0 = batch.stats()
-        with torch.cuda.stream(stream):
-            for _ in range(args.settle + args.warmup + min(steps, 64)):
-                one_step()
-        torch.cuda.synchronize()
-        s1 = batch.stats()
+        # the same run once more with the skipped tests executed and checked (the shortened
+        # summaries skip the audits: their lockstep event comparison checks the learned path)
+        audit = not getattr(args, "summary", False)
+
+        def audited(mode):
+            if not audit:
+                return None, None
+            start(mode)
+            a0 = batch.stats()
+            with torch.cuda.stream(stream):
+                for _ in range(args.settle + args.warmup + min(steps, 64)):
+                    one_step()
+            torch.cuda.synchronize()
+            a1 = batch.stats()
+            return a1["missed_contacts"] - a0["missed_contacts"], a1["arenas_reverted"]
+
+        missed, reverted = audited(rsb.RSB_CULL_LEARNED_AUDIT)
         tested = queries["culled_queries"] + queries["narrowphase_queries"]
         # the same rollout with the bound that needs no training (voxel distance field)
         start(rsb.RSB_CULL_VOXEL)
         warm()
         vx_value, vx_ms, vx_steps, vx_q = timed(steps, [])
-        start(rsb.RSB_CULL_VOXEL_AUDIT)
-        s2 = batch.stats()
-        with torch.cuda.stream(stream):
-            for _ in range(args.settle + args.warmup + min(steps, 64)):
-                one_step()
-        torch.cuda.synchronize()
-        s3 = batch.stats()
+        vx_missed, _ = audited(rsb.RSB_CULL_VOXEL_AUDIT)
         vx_tested = vx_q["culled_queries"] + vx_q["narrowphase_queries"]
         learned = {"train": culler, "culled_fraction": queries["culled_queries"] / max(1, tested),
-                   "static_tests": queries, "audit_missed_contacts": s1["missed_contacts"] - s0["missed_contacts"],
-                   "audit_arenas_reverted": s1["arenas_reverted"],
+                   "static_tests": queries, "audit_missed_contacts": missed,
+                   "audit_arenas_reverted": reverted,
                    "exact_bvh": {"value": ex_value, "ms_per_step": ex_ms / steps,
                                  "kernel_ms": statistics.mean(ex_steps), "static_tests": ex_q},
                    "learned_over_exact": value / ex_value,
                    "voxel_bound": {"value": vx_value, "ms_per_step": vx_ms / steps,
                                    "kernel_ms": statistics.mean(vx_steps),
                                    "culled_fraction": vx_q["culled_queries"] / max(1, vx_tested),
-                                   "audit_missed_contacts": s3["missed_contacts"] - s2["missed_contacts"],
+                                   "audit_missed_contacts": vx_missed,
                                    "over_exact": vx_value / ex_value}}
         batch.set_cull_mode(rsb.RSB_CULL_LEARNED)
     if wl.preset == "c4":
-        extra["stress"] = stress_events(pkg, batch, wl, rank, dev)
-        extra["stress"]["solver_rows_per_arena_tick"] = queries["solver_rows"] / (wl.num_arenas * wl.tick_skip * steps)
+        # the full 4,096-tick rollout; the folded summary of the headline line runs it on a
+        # quarter of the arenas
+        extra["stress"] = stress_events(pkg, batch, wl, rank, dev, 4096 // wl.tick_skip,
+                                        wl.num_arenas // 4 if getattr(args, "summary", False) else None)
 
     # e2e through the public API with host buffers, as the collector's host path runs it:
     # host actions in (H2D), step, obs / masks / rewards / terminals back to the host (D2H),
@@ -475,7 +480,7 @@ def run_ours(args, rank, world, dist):
     # the reference's own GPU batch (RocketSimCuda's stepArenaKernel and env kernels, built for
     # sm_100a) on the same settled state and a seeded action stream, timed the same way
     refgpu = None
-    if wl.preset == "c3" and not args.no_ref_gpu and rank == 0:
+    if wl.preset == "c3" and not args.no_ref_gpu and world == 1:
         refgpu = reference_gpu(batch, wl, lut, pkg.MESHES_DIR, args.steps, args.warmup, args.settle)
 
     # roofline of the step kernel (the dominant launch): algorithmic bytes = persistent
@@ -664,18 +669,21 @@ def reference_gpu_drift(pkg, lib, meshes, n=256, ticks=120, seed=0x5EED0006):
         eng.close()
 
 
-def stress_events(pkg, trained, wl, rank, dev):
-    """Goal and demo events of 64 env steps on the exact and on the learned path, run in
-    lockstep on two fresh batches built the same way (same seeds, same actions), step by
-    step (goals: terminal flag 1; demoed cars: the demo flag of the obs rows)."""
+def stress_events(pkg, trained, wl, rank, dev, steps, arenas=None):
+    """Goal and demo events of `steps` env steps (512 = one 4,096-tick rollout at tickSkip 8)
+    on the exact and on the learned path, run in lockstep on two fresh batches of `arenas`
+    arenas built the same way (same seeds, same actions), step by step (goals: terminal flag
+    1; demoed cars: the demo flag of the obs rows); finished arenas reset on the device with
+    the workload's reset mode, the same seed on both sides."""
     import torch
     rsb = pkg.rsb
     weights, margin = trained.culler_get()
     lut = rsb.default_action_lut(trained.lib)
     w = wl.action_weights(lut)
+    n = arenas or wl.num_arenas
     mk = []
     for mode in (rsb.RSB_CULL_EXACT, rsb.RSB_CULL_LEARNED):
-        b = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size or None,
+        b = rsb.Batch(pkg.engine_library(), n, team_size=wl.team_size or None,
                       team_sizes=wl.team_sizes(), meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank,
                       rewards=rsb.default_rewards(pkg.engine_library(), episode_max_ticks=EPISODE_TICKS),
                       cull_mode=mode)
@@ -684,11 +692,12 @@ def stress_events(pkg, trained, wl, rank, dev):
             b.culler_set(weights, margin)
         b.reset_all(0x5EED0001 + rank, wl.reset_mode(rsb))
         obs = torch.as_tensor(DevArray(b.device_ptr(rsb.RSB_BUF_OBS), (b.num_cars, b.obs_stride), "<f4"), device=dev)
-        term = torch.as_tensor(DevArray(b.device_ptr(rsb.RSB_BUF_TERMINALS), (wl.num_arenas,), "|u1"), device=dev)
+        term = torch.as_tensor(DevArray(b.device_ptr(rsb.RSB_BUF_TERMINALS), (n,), "|u1"), device=dev)
         mk.append((b, obs, term))
     rng = np.random.default_rng(0x5EED0006 + rank)
     seqs = [[], []]
-    for step in range(64):
+    s0 = [b.stats() for b, _, _ in mk]
+    for step in range(steps):
         idx = rng.choice(len(lut), mk[0][0].num_cars, p=w).astype(np.int32)
         for k, (b, obs, term) in enumerate(mk):
             b.set_actions(idx)
@@ -700,12 +709,54 @@ def stress_events(pkg, trained, wl, rank, dev):
             b.reset_done(0x5EED4000 + step, wl.reset_mode(rsb))
     same_state = (mk[0][0].get_cars().tobytes() == mk[1][0].get_cars().tobytes() and
                   mk[0][0].get_balls().tobytes() == mk[1][0].get_balls().tobytes())
-    learned_stats = mk[1][0].stats()
+    s1 = [b.stats() for b, _, _ in mk]
     ex, le = seqs
-    return {"steps_compared": len(ex), "goals_exact": sum(g for g, _ in ex), "goals_learned": sum(g for g, _ in le),
+    dq = [{k: s1[i][k] - s0[i][k] for k in ("culled_queries", "narrowphase_queries", "solver_rows")} for i in (0, 1)]
+    for b, _, _ in mk:
+        b.close()
+    return {"arenas": n, "steps_compared": len(ex), "ticks": len(ex) * wl.tick_skip,
+            "goals_exact": sum(g for g, _ in ex), "goals_learned": sum(g for g, _ in le),
             "demoed_car_steps_exact": sum(d for _, d in ex), "demoed_car_steps_learned": sum(d for _, d in le),
             "event_agreement": sum(a == b for a, b in zip(ex, le)) / len(ex), "final_state_identical": same_state,
-            "culled_queries": learned_stats["culled_queries"]}
+            "culled_queries": dq[1]["culled_queries"],
+            "culled_fraction": dq[1]["culled_queries"] / max(1, dq[1]["culled_queries"] + dq[1]["narrowphase_queries"]),
+            "solver_rows_per_arena_tick": dq[0]["solver_rows"] / (n * wl.tick_skip * len(ex))}
+
+
+def config_summaries(args, rank, world, dist):
+    """The three other workloads, shortened, folded into the headline line: c1 and c2 (c2
+    replaying the library's captured env step) with the headline's timed steps, c4 with the
+    same timed steps and its lockstep exact-vs-learned event comparison over one full
+    4,096-tick rollout on a quarter of its arenas (32,768), so that the whole line ends within
+    a few minutes (`--config c4` runs the rollout at full size).  Each carries the reference's
+    CPU rate on a short sample of the same workload."""
+    import gc
+    out = {}
+    for name in ("c1", "c2", "c4"):
+        a = argparse.Namespace(**vars(args))
+        a.config, a.arenas, a.team_size, a.cull, a.summary = name, None, None, None, True
+        a.no_ring = a.no_pred = a.no_obs_roofline = a.no_ref_gpu = True
+        r = run_ours(a, rank, world, dist)
+        gc.collect()
+        s = {"workload": r["config"]["workload"], "value": r["value"], "unit": r["unit"], "steps": r["steps"],
+             "ms_per_step": r["ms_per_step"], "e2e": r["e2e"]["value"], "gpu_launches": r["gpu_launches"],
+             "step_kernel_ms": r["roofline"]["kernel_ms"], "clocks": r["clocks"]}
+        for k in ("graph", "stress"):
+            if k in r:
+                s[k] = r[k]
+        if r.get("learned_cull"):
+            lc = r["learned_cull"]
+            s["learned_cull"] = {"learned_over_exact": lc["learned_over_exact"], "exact_value": lc["exact_bvh"]["value"],
+                                 "culled_fraction": lc["culled_fraction"],
+                                 "audit_missed_contacts": lc["audit_missed_contacts"],
+                                 "voxel_over_exact": lc["voxel_bound"]["over_exact"],
+                                 "voxel_culled_fraction": lc["voxel_bound"]["culled_fraction"]}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            ref = cpu_reference(a, sample_s=4.0)
+            s["reference_cpu"] = {"value": ref["value"], "cores": ref["cores"], "sample": ref["sample"]}
+            s["vs_reference_cpu"] = r["value"] / ref["value"]
+        out[name] = s
+    return out
 
 
 # ------------------------------------------------------------------ GAE over a rollout buffer
@@ -944,6 +995,8 @@ def main():
     ap.add_argument("--no-obs-roofline", action="store_true", help="skip timing the observation kernel alone")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference's own GPU batch in the c3 line")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the shortened c1 / c2 / c4 summaries of the c3 line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -972,6 +1025,8 @@ def main():
     # the next stage of the rollout: GAE over a rollout buffer of this size, device-resident
     if args.config == "c3" and not args.no_gae:
         res["gae"] = run_gae(args, rank, world, dist, steps=10, warmup=3)
+    if args.config == "c3" and world == 1 and not args.no_configs:
+        res["configs"] = config_summaries(args, rank, world, dist)
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             res["cpu_baseline"] = cpu_reference(args, sample_s=args.ref_seconds)

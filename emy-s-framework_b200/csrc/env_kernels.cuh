@@ -186,7 +186,7 @@ RSB_D uint32_t maskNibbleBytes(uint32_t m0, uint32_t m1, uint32_t m2, int b) {
 //   C. send the staged rows out: the 16-byte-aligned middle as one bulk copy from shared
 //      memory (cp.async.bulk), the few elements either side as plain stores.
 constexpr int OBS_THREADS = 256;
-__global__ void __launch_bounds__(OBS_THREADS) obsKernel(EnvView E, EnvTables Tb) {
+__global__ void __launch_bounds__(OBS_THREADS, 6) obsKernel(EnvView E, EnvTables Tb) {
     __shared__ ObsShared S;
     const int tid = threadIdx.x;
     const int a0 = blockIdx.x * OBS_ARENAS;

@@ -65,7 +65,13 @@ struct EnvView {
     uint8_t* masks;
     float* rewards;
     uint8_t* terminals;
+    uint32_t* vantaArena;  // VantaObs builder state (VANTA_ARENA_WORDS planes), null when off
+    uint32_t* vantaCar;    // VANTA_CAR_WORDS planes of [MAX_CARS][N]
 };
+// Words of the VantaObs builder's state per arena and per car (laid out in vanta.cuh); an arena
+// reset clears them, as the reference's ResetArena clears the builder's state
+// (RocketSimCudaApi.cuh:265-275).
+constexpr int VANTA_ARENA_WORDS = NUM_PADS + 5, VANTA_CAR_WORDS = 13;
 
 // word indices inside the records
 #define RSB_W(T, f) ((int)(offsetof(T, f) / 4))
@@ -541,6 +547,10 @@ __global__ void resetKernel(EnvView E, EnvTables Tb, ResetCurriculum Cu, const i
     if (seedPtr) seed = *seedPtr;  // a replayed graph reads the seed of this launch from the device
     const int a = idx ? idx[i] : i;
     if (onlyDone && E.terminals[a] == 0) return;
+    if (E.vantaArena) {
+        for (int w = 0; w < VANTA_ARENA_WORDS; w++) E.vantaArena[(size_t)w * E.N + a] = 0u;
+        for (int w = 0; w < VANTA_CAR_WORDS * MAX_CARS; w++) E.vantaCar[(size_t)w * E.N + a] = 0u;
+    }
     const int T = E.teamSize[a], M = 2 * T, base = E.carOffset[a];
     ResetRng g{seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(a + 1)), 0};
     constexpr float PI = 3.14159265358979323846f;

@@ -22,6 +22,7 @@
 #include "engine_host.h"
 #include "env_kernels.cuh"
 #include "culler.cuh"
+#include "vanta.cuh"
 
 #include <numeric>
 #include <random>
@@ -140,6 +141,13 @@ struct rsb_handle {
     size_t predCap = 0;
     size_t stageWords = 0;
     EnvTables tables{};
+    // VantaObs builder (rsb_vanta_configure)
+    uint32_t* dVA = nullptr;
+    uint32_t* dVT = nullptr;
+    rsb_ball_state* dVantaPred = nullptr;
+    float* dVantaRows = nullptr;
+    rsb_vanta_config vanta{};
+    VantaTables vantaTables{};
     // captured env step (rsb_env_graph_capture)
     cudaGraphExec_t envGraph = nullptr;
     uint64_t* dGraphSeed = nullptr;
@@ -462,6 +470,8 @@ static EnvView envView(rsb_handle* h) {
     E.masks = h->dMasks;
     E.rewards = h->dRewards;
     E.terminals = h->dTerminals;
+    E.vantaArena = h->dVA;
+    E.vantaCar = h->dVT;
     return E;
 }
 
@@ -667,6 +677,10 @@ rsb_status rsb_destroy(rsb_handle* h) {
     cudaFree(h->dCw); cudaFree(h->dCwBf); cudaFree(h->dCull); cudaFree(h->dCounters); cudaFree(h->dLog);
     cudaFree(h->dTris);
     cudaFree(h->dObs); cudaFree(h->dMasks); cudaFree(h->dRewards); cudaFree(h->dTerminals); cudaFree(h->dResetIdx);
+    cudaFree(h->dVA);
+    cudaFree(h->dVT);
+    cudaFree(h->dVantaPred);
+    cudaFree(h->dVantaRows);
     if (h->envGraph) cudaGraphExecDestroy(h->envGraph);
     cudaFree(h->dGraphSeed);
     cudaFree(h->ring.dSlots); cudaFree(h->ring.dJobs); cudaFree(h->dStage); cudaFree(h->dWork); cudaFree(h->dPred);
@@ -1727,6 +1741,7 @@ rsb_status rsb_device_ptr(rsb_handle* h, int32_t which, void** out) {
         case RSB_BUF_CONTROLS: *out = h->dControls; return RSB_OK;
         case RSB_BUF_ACTIONS: *out = h->dActions; return RSB_OK;
         case RSB_BUF_BALL_PRED: *out = h->dPred; return RSB_OK;
+        case RSB_BUF_VANTA_OBS: *out = h->dVantaRows; return RSB_OK;
         default: return fail(h, RSB_ERR_INVALID, "unknown buffer");
     }
 }
@@ -1764,6 +1779,112 @@ rsb_status rsb_reset_done(rsb_handle* h, uint64_t seed, int32_t mode, void* stre
     resetKernel<<<(h->N + 127) / 128, 128, 0, pick(h, stream)>>>(envView(h), h->tables, h->curriculum, nullptr, h->N,
                                                                   seed, mode, true);
     RSB_CUDA(cudaGetLastError());
+    return RSB_OK;
+}
+
+static rsb_status copyOut(rsb_handle* h, void* out, const void* dev, size_t count, size_t expect, size_t elem,
+                          const char* what);
+
+rsb_status rsb_vanta_default_config(rsb_vanta_config* cfg) {
+    if (!cfg) return RSB_ERR_INVALID;
+    *cfg = rsb_vanta_config{};
+    cfg->tick_skip = 8;
+    cfg->dodge_deadzone = 0.5f;
+    cfg->only_closest_opp = 0;
+    cfg->predict_ball = 1;
+    return RSB_OK;
+}
+
+rsb_status rsb_vanta_configure(rsb_handle* h, const rsb_vanta_config* cfg) {
+    if (!h || !cfg || cfg->tick_skip <= 0 || !(cfg->dodge_deadzone >= 0.f))
+        return fail(h, RSB_ERR_INVALID, "bad VantaObs configuration");
+    RSB_CUDA(cudaSetDevice(h->device));
+    const size_t N = h->N;
+    if (!h->dVA) {
+        if (cudaMalloc((void**)&h->dVA, (size_t)VA_WORDS * N * 4) != cudaSuccess ||
+            cudaMalloc((void**)&h->dVT, (size_t)VT_WORDS * MAX_CARS * N * 4) != cudaSuccess ||
+            cudaMalloc((void**)&h->dVantaPred, N * 3 * sizeof(rsb_ball_state)) != cudaSuccess ||
+            cudaMalloc((void**)&h->dVantaRows, std::max<size_t>(1, h->numCars) * VANTA_ROW * 4) != cudaSuccess) {
+            cudaFree(h->dVA); cudaFree(h->dVT); cudaFree(h->dVantaPred); cudaFree(h->dVantaRows);
+            h->dVA = h->dVT = nullptr;
+            h->dVantaPred = nullptr;
+            h->dVantaRows = nullptr;
+            return fail(h, RSB_ERR_NOMEM, "VantaObs state allocation failed");
+        }
+    }
+    // a (re)configured builder starts from its default state, as after a reset
+    RSB_CUDA(cudaMemsetAsync(h->dVA, 0, (size_t)VA_WORDS * N * 4, h->stream));
+    RSB_CUDA(cudaMemsetAsync(h->dVT, 0, (size_t)VT_WORDS * MAX_CARS * N * 4, h->stream));
+    RSB_CUDA(cudaMemsetAsync(h->dVantaRows, 0, std::max<size_t>(1, h->numCars) * VANTA_ROW * 4, h->stream));
+    // pad tables in RLGym order (the AdvancedObs pad map), z of the pad table, and the
+    // x-mirror permutation: the first pad at (-x, y, z) within 1 uu (RocketSimCudaHostUtils.cuh:66-86)
+    VantaTables& T = h->vantaTables;
+    for (int i = 0; i < NUM_PADS; i++) {
+        const PadLoc& l = PAD_LOCS_HOST[h->tables.padMap[i]];
+        T.x[i] = l.x;
+        T.y[i] = l.y;
+        T.z[i] = l.z;
+        T.pad[i] = (uint8_t)h->tables.padMap[i];
+    }
+    for (int i = 0; i < NUM_PADS; i++) {
+        int m = i;
+        for (int j = 0; j < NUM_PADS; j++)
+            if (std::fabs(T.x[j] + T.x[i]) < 1.f && std::fabs(T.y[j] - T.y[i]) < 1.f && std::fabs(T.z[j] - T.z[i]) < 1.f) {
+                m = j;
+                break;
+            }
+        T.mirror[i] = (uint8_t)m;
+    }
+    h->vanta = *cfg;
+    RSB_CUDA(cudaStreamSynchronize(h->stream));
+    return RSB_OK;
+}
+
+rsb_status rsb_build_vanta_obs(rsb_handle* h, void* stream) {
+    if (!h) return RSB_ERR_INVALID;
+    if (!h->dVA) return fail(h, RSB_ERR_STATE, "VantaObs is not configured (rsb_vanta_configure)");
+    RSB_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = pick(h, stream);
+    VantaView V{};
+    V.arena = h->dVA;
+    V.car = h->dVT;
+    V.rows = h->dVantaRows;
+    V.dt = (float)h->vanta.tick_skip / 120.f;
+    V.deadzone = h->vanta.dodge_deadzone;
+    V.onlyClosestOpp = h->vanta.only_closest_opp;
+    if (h->vanta.predict_ball) {
+        // the ball-only rollout of BallPredTracker, slices at 1, 2 and 3 s
+        PredSlices ps{};
+        ps.n = 3;
+        ps.t[0] = 120;
+        ps.t[1] = 240;
+        ps.t[2] = 360;
+        predictBallKernel<<<(h->N + 127) / 128, 128, 0, st>>>(devView(h), ps, h->dVantaPred);
+        RSB_CUDA(cudaGetLastError());
+        V.pred = h->dVantaPred;
+    }
+    const EnvView E = envView(h);
+    vantaArenaKernel<<<(h->N + 127) / 128, 128, 0, st>>>(E, V, h->vantaTables);
+    RSB_CUDA(cudaGetLastError());
+    if (h->numCars > 0) {
+        vantaRowKernel<<<(h->numCars + 127) / 128, 128, 0, st>>>(E, V, h->vantaTables, h->numCars);
+        RSB_CUDA(cudaGetLastError());
+    }
+    return RSB_OK;
+}
+
+rsb_status rsb_copy_vanta_obs(rsb_handle* h, float* out, size_t n) {
+    if (h && !h->dVantaRows) return fail(h, RSB_ERR_STATE, "VantaObs is not configured (rsb_vanta_configure)");
+    return copyOut(h, out, h ? h->dVantaRows : nullptr, n, h ? (size_t)h->numCars * VANTA_ROW : 0, 4, "vanta obs");
+}
+
+rsb_status rsb_pad_locations(float* xyz) {
+    if (!xyz) return RSB_ERR_INVALID;
+    for (int p = 0; p < NUM_PADS; p++) {
+        xyz[3 * p + 0] = PAD_LOCS_HOST[p].x;
+        xyz[3 * p + 1] = PAD_LOCS_HOST[p].y;
+        xyz[3 * p + 2] = PAD_LOCS_HOST[p].z;
+    }
     return RSB_OK;
 }
 

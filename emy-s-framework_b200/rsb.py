@@ -27,7 +27,9 @@ RSB_STATIC_ACTIONS_MAX = 65536 * 6
 RSB_OBS_BASE = 51
 RSB_OBS_PER_CAR = 29
 
-RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS, RSB_BUF_BALL_PRED = range(7)
+(RSB_BUF_OBS, RSB_BUF_MASKS, RSB_BUF_REWARDS, RSB_BUF_TERMINALS, RSB_BUF_CONTROLS, RSB_BUF_ACTIONS, RSB_BUF_BALL_PRED,
+ RSB_BUF_VANTA_OBS) = range(8)
+RSB_VANTA_OBS_SIZE = 366
 RSB_MAX_PRED_SLICES = 8
 RSB_MAX_PRED_TICKS = 4096
 RSB_CULL_EXACT, RSB_CULL_LEARNED, RSB_CULL_LEARNED_AUDIT, RSB_CULL_VOXEL, RSB_CULL_VOXEL_AUDIT = 0, 1, 2, 3, 4
@@ -162,6 +164,11 @@ class Stats(C.Structure):
         "solver_rows", "arenas_reverted", "status_bits_seen", "state_bytes_per_step")]
 
 
+class VantaConfig(C.Structure):
+    _fields_ = [("tick_skip", C.c_int32), ("dodge_deadzone", C.c_float), ("only_closest_opp", C.c_int32),
+                ("predict_ball", C.c_int32)]
+
+
 class RingConfig(C.Structure):
     _fields_ = [("depth", C.c_int32), ("capture_every", C.c_int32), ("restore_fraction", C.c_float),
                 ("max_arenas_per_restore", C.c_int32), ("fuzz_pos", C.c_float), ("fuzz_vel", C.c_float),
@@ -254,6 +261,11 @@ _SIGS = {
     "rsb_eval_refmath": [C.c_int32, _P, _P, _P, C.c_int64, C.c_int32],
     "rsb_set_reset_curriculum": [_P, C.c_float, C.c_float, C.c_float, C.c_float],
     "rsb_env_graph_capture": [_P, _P, C.c_int32, C.c_int32, C.c_uint64],
+    "rsb_vanta_default_config": [C.POINTER(VantaConfig)],
+    "rsb_vanta_configure": [_P, C.POINTER(VantaConfig)],
+    "rsb_build_vanta_obs": [_P, _P],
+    "rsb_copy_vanta_obs": [_P, _P, C.c_size_t],
+    "rsb_pad_locations": [_P],
     "rsb_env_graph_launch": [_P, _P],
 }
 
@@ -298,6 +310,15 @@ def default_rewards(lib: C.CDLL, **overrides) -> RewardConfig:
     for k, v in overrides.items():
         setattr(r, k, v)
     return r
+
+
+def pad_locations(lib: C.CDLL) -> np.ndarray:
+    """rsb_pad_locations: the 34 pad locations (x, y, z) in the order of the pad-state arrays."""
+    out = np.zeros((RSB_NUM_PADS, 3), np.float32)
+    st = lib.rsb_pad_locations(_ptr(out))
+    if st != 0:
+        raise RsbError(st, _global_error(lib))
+    return out
 
 
 def default_action_lut(lib: C.CDLL) -> np.ndarray:
@@ -523,6 +544,24 @@ class Batch:
 
     def env_graph_launch(self, stream: int | None = None):
         self._check(self.lib.rsb_env_graph_launch(self._h, C.c_void_p(stream or 0)))
+
+    def vanta_configure(self, **overrides) -> VantaConfig:
+        """rsb_vanta_configure with the reference's defaults (tickSkip 8, dodge deadzone 0.5, all
+        three opponents, ball prediction on) and the given fields; clears the builder's state."""
+        cfg = VantaConfig()
+        self._check_global(self.lib.rsb_vanta_default_config(C.byref(cfg)))
+        for k, v in overrides.items():
+            setattr(cfg, k, v)
+        self._check(self.lib.rsb_vanta_configure(self._h, C.byref(cfg)))
+        return cfg
+
+    def build_vanta_obs(self, stream: int | None = None):
+        self._check(self.lib.rsb_build_vanta_obs(self._h, C.c_void_p(stream or 0)))
+
+    def copy_vanta_obs(self) -> np.ndarray:
+        out = np.zeros((self.num_cars, RSB_VANTA_OBS_SIZE), np.float32)
+        self._check(self.lib.rsb_copy_vanta_obs(self._h, _ptr(out), out.size))
+        return out
 
     def set_reset_curriculum(self, kickoff_w: float, fuzzed_w: float, aerial_w: float, chase_w: float = 0.0):
         self._check(self.lib.rsb_set_reset_curriculum(self._h, kickoff_w, fuzzed_w, aerial_w, chase_w))

@@ -84,7 +84,8 @@ enum {
                                (goal), 2 truncated (no touch / episode tick limit) */
     RSB_BUF_CONTROLS = 4,   /* rsb_controls [num_cars] */
     RSB_BUF_ACTIONS = 5,    /* int32 [num_cars] */
-    RSB_BUF_BALL_PRED = 6   /* rsb_ball_state [num_arenas][n_slices] of the last rsb_predict_ball */
+    RSB_BUF_BALL_PRED = 6,  /* rsb_ball_state [num_arenas][n_slices] of the last rsb_predict_ball */
+    RSB_BUF_VANTA_OBS = 7   /* float [num_cars][RSB_VANTA_OBS_SIZE] of the last rsb_build_vanta_obs */
 };
 
 /* Arena-narrowphase mode. */
@@ -268,6 +269,30 @@ rsb_status rsb_layout(const rsb_handle* h, int32_t* num_arenas, int32_t* num_car
 rsb_status rsb_obs_stride(const rsb_handle* h, int32_t* stride);
 
 rsb_status rsb_reset_all(rsb_handle* h, uint64_t seed, int32_t mode);
+/* VantaObs v3.5 rows (RocketSimCudaBatch::BuildVantaObs, RocketSimCuda.h:318-321, the device
+ * builder VantaObsGpu.cuh): 366 floats per player, packed like the AdvancedObs rows
+ * (row = rsb_layout's car offset of the arena + creation slot).  The builder keeps state
+ * between builds: boost-pad timers per arena and demo / action timers per player, each
+ * updated once per arena tick; an arena reset clears that arena's state
+ * (RocketSimCudaApi.cuh:265-275).  With predict_ball the ball block carries the ball-only
+ * rollout's positions and velocities at 120 / 240 / 360 ticks (as rsb_predict_ball), else
+ * zeros.  Configuring (again) allocates the state once and clears it. */
+#define RSB_VANTA_OBS_SIZE 366
+typedef struct rsb_vanta_config {
+    int32_t tick_skip;        /* the timers' step: tick_skip / 120 s (BatchConfig::vantaTickSkip, 8) */
+    float dodge_deadzone;     /* BatchConfig::vantaDodgeDeadzone, 0.5 */
+    int32_t only_closest_opp; /* BatchConfig::vantaOnlyClosestOpp, 0 */
+    int32_t predict_ball;     /* BatchConfig::vantaPredictBall (default here 1) */
+} rsb_vanta_config;
+rsb_status rsb_vanta_default_config(rsb_vanta_config* cfg);
+rsb_status rsb_vanta_configure(rsb_handle* h, const rsb_vanta_config* cfg);
+/* Builds every player's row from the current state, on `stream` (NULL = the handle's). */
+rsb_status rsb_build_vanta_obs(rsb_handle* h, void* stream);
+/* n = num_cars * RSB_VANTA_OBS_SIZE; synchronises the handle's stream. */
+rsb_status rsb_copy_vanta_obs(rsb_handle* h, float* out, size_t n);
+/* The 34 boost-pad locations (x, y, z in uu) in the order of rsb_pad_state arrays. */
+rsb_status rsb_pad_locations(float* xyz);
+
 /* One collector env step captured as a CUDA graph (the reference launches each kernel of a
  * step separately, RocketSimCudaApi.cuh:551-571; no counterpart there): action expansion from
  * d_actions (device int32 [num_cars], read at every launch, so the caller refills it in

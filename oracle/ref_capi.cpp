@@ -1072,6 +1072,35 @@ rsb_status rsb_set_reset_curriculum(rsb_handle* h, float, float, float, float) {
     return h ? RSB_OK : RSB_ERR_INVALID;
 }
 
+// The VantaObs builder is checked against the reference's own device builder
+// (oracle/vanta_pin.cu), not against this library.
+rsb_status rsb_vanta_default_config(rsb_vanta_config* cfg) {
+    if (!cfg) return RSB_ERR_INVALID;
+    *cfg = rsb_vanta_config{8, 0.5f, 0, 1};
+    return RSB_OK;
+}
+rsb_status rsb_vanta_configure(rsb_handle* h, const rsb_vanta_config*) {
+    return fail(h, RSB_ERR_UNSUPPORTED, "the CPU oracle has no VantaObs builder");
+}
+rsb_status rsb_build_vanta_obs(rsb_handle* h, void*) {
+    return fail(h, RSB_ERR_UNSUPPORTED, "the CPU oracle has no VantaObs builder");
+}
+rsb_status rsb_copy_vanta_obs(rsb_handle* h, float*, size_t) {
+    return fail(h, RSB_ERR_UNSUPPORTED, "the CPU oracle has no VantaObs builder");
+}
+// Arena's pads: the big soccar pads, then the small ones (Arena.cpp:546-550).
+rsb_status rsb_pad_locations(float* xyz) {
+    if (!xyz) return RSB_ERR_INVALID;
+    using namespace RocketSim::RLConst::BoostPads;
+    for (int i = 0; i < LOCS_AMOUNT_BIG + LOCS_AMOUNT_SMALL_SOCCAR; i++) {
+        const RocketSim::Vec& v = i < LOCS_AMOUNT_BIG ? LOCS_BIG_SOCCAR[i] : LOCS_SMALL_SOCCAR[i - LOCS_AMOUNT_BIG];
+        xyz[3 * i + 0] = v.x;
+        xyz[3 * i + 1] = v.y;
+        xyz[3 * i + 2] = v.z;
+    }
+    return RSB_OK;
+}
+
 // CUDA graphs have no counterpart on the CPU oracle.
 rsb_status rsb_env_graph_capture(rsb_handle* h, const int32_t*, int32_t, int32_t, uint64_t) {
     return fail(h, RSB_ERR_UNSUPPORTED, "no CUDA graphs on the CPU oracle");

@@ -64,3 +64,25 @@ def test_default_action_table_shape(pkg):
     assert (air["throttle"] == air["boost"]).all() and (air["steer"] == air["yaw"]).all()
     assert not ((air["jump"] == 1) & (air["yaw"] != 0)).any()
     assert len(np.unique(lut.tobytes())) == 1 and len({r.tobytes() for r in lut}) == 90
+
+
+def test_pad_locations_match_reference(pkg):
+    """The engine's pad order and locations (rsb_pad_locations) are RocketSim's arena pads:
+    the big soccar pads, then the small ones (Arena.cpp:546-550), as the oracle reports them."""
+    rsb = pkg.rsb
+    a = rsb.pad_locations(pkg.engine_library())
+    b = rsb.pad_locations(rsb.load_library(ORACLE_LIB))
+    assert a.shape == (rsb.RSB_NUM_PADS, 3) and a.tobytes() == b.tobytes()
+    assert (a[:6, 2] == 73).all() and (a[6:, 2] == 70).all()
+
+
+def test_vanta_default_config(pkg):
+    """BatchConfig's VantaObs defaults (RocketSimCuda.h:184-189) from both libraries, ball
+    prediction on."""
+    import ctypes as C
+
+    rsb = pkg.rsb
+    for lib in (pkg.engine_library(), rsb.load_library(ORACLE_LIB)):
+        cfg = rsb.VantaConfig()
+        assert lib.rsb_vanta_default_config(C.byref(cfg)) == 0
+        assert (cfg.tick_skip, cfg.dodge_deadzone, cfg.only_closest_opp, cfg.predict_ball) == (8, 0.5, 0, 1)

@@ -477,6 +477,29 @@ def run_ours(args, rank, world, dist):
                "frac": ach / peak, "bytes_per_call": out_b + in_b, "ms": oms, "traffic": None,
                "l2": "flushed by a 256 MB write, then a read of it, before each call"}
 
+    # VantaObs rows (rsb_build_vanta_obs) of every player, without and with the ball-only
+    # prediction rollout the builder runs (360 ticks, slices at 1 / 2 / 3 s), L2 flushed the same
+    # way; bytes: the rows written
+    vanta = None
+    if wl.preset == "c3" and not args.no_obs_roofline:
+        vanta = {"players": batch.num_cars, "row_floats": rsb.RSB_VANTA_OBS_SIZE}
+        for pred_on in (0, 1):
+            batch.vanta_configure(predict_ball=pred_on)
+            vms = []
+            with torch.cuda.stream(stream):
+                for k in range(5):
+                    flush.fill_(1.0)
+                    flush.sum()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    batch.build_vanta_obs(stream=sp)
+                    e1.record(stream)
+                    e1.synchronize()
+                    vms.append(e0.elapsed_time(e1))
+            ms = statistics.median(vms[1:])
+            key = "with_ball_prediction" if pred_on else "rows_only"
+            vanta[key] = {"ms": ms, "rows_gbs": batch.num_cars * rsb.RSB_VANTA_OBS_SIZE * 4 / ms / 1e6}
+
     # the reference's own GPU batch (RocketSimCuda's stepArenaKernel and env kernels, built for
     # sm_100a) on the same settled state and a seeded action stream, timed the same way
     refgpu = None
@@ -516,6 +539,7 @@ def run_ours(args, rank, world, dist):
         "ball_prediction": pred,
         "reference_gpu": refgpu,
         "obs_roofline": obs,
+        "vanta_obs": vanta,
         "autotune": tune,
         "clocks": clocks[-1],
         "clocks_exact": clocks[0],

@@ -116,7 +116,7 @@ RSB_HD int obsCarIndex(int T, int p, int q) {
 }
 
 // Per-arena inputs of the car blocks, staged in shared memory, one column per arena.
-constexpr int OBS_ARENAS = 4;
+constexpr int OBS_ARENAS = 8;
 constexpr int OI_BALL = 0;                        // ball pos, vel (uu)
 constexpr int OI_CAR = 6;                         // per car, OI_CAR_N words
 constexpr int OI_CAR_N = 21;                      // pos vel ang fwd right up boost flags, 1 pad word
@@ -181,9 +181,10 @@ RSB_D uint32_t maskNibbleBytes(uint32_t m0, uint32_t m1, uint32_t m2, int b) {
     return (x * 0x00204081u) & 0x01010101u;
 }
 
-// A block of 256 threads serves 4 arenas (24 KB of shared memory) in three phases, every
-// thread taking part in each, one item per thread where the items allow (so that a thread's
-// reads are issued together, not behind one another):
+// A block of 512 threads serves 8 arenas (47 KB of shared memory, at most 40 registers a
+// thread: 3 blocks per SM) in three phases, every thread taking part in each, one item per
+// thread where the items allow (so that a thread's reads are issued together, not behind one
+// another):
 //   A. read the arenas' word planes (consecutive threads on consecutive arenas of one word),
 //      stage what the car blocks need, and write the ball, action and pad columns of every
 //      row straight into the staged rows;
@@ -191,8 +192,8 @@ RSB_D uint32_t maskNibbleBytes(uint32_t m0, uint32_t m1, uint32_t m2, int b) {
 //      and the mask bytes of the block's rows to the output as 32-bit words;
 //   C. send the staged rows out: the 16-byte-aligned middle as one bulk copy from shared
 //      memory (cp.async.bulk), the few elements either side as plain stores.
-constexpr int OBS_THREADS = 256;
-__global__ void __launch_bounds__(OBS_THREADS, 6) obsKernel(EnvView E, EnvTables Tb) {
+constexpr int OBS_THREADS = 512;
+__global__ void __launch_bounds__(OBS_THREADS, 3) obsKernel(EnvView E, EnvTables Tb) {
     __shared__ ObsShared S;
     const int tid = threadIdx.x;
     const int a0 = blockIdx.x * OBS_ARENAS;

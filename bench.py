@@ -134,10 +134,23 @@ class Workload:
         self.tick_skip = args.tick_skip
         self.desc = p["desc"]
 
+        self.offset, self.global_arenas, self.strong = 0, self.num_arenas, False
+
     def team_sizes(self):
         if self.mixed:
-            return np.array([1 + (a % 3) for a in range(self.num_arenas)], np.int32)
+            return np.array([1 + ((self.offset + a) % 3) for a in range(self.num_arenas)], np.int32)
         return None
+
+    def shard(self, rank, world):
+        """Strong scaling: this rank's contiguous range of the preset's arenas, the ranges
+        balanced by car count (shard_range)."""
+        full = np.array([1 + (a % 3) for a in range(self.global_arenas)], np.int32) if self.mixed else None
+        lo, hi = shard_range(full, self.global_arenas, rank, world)
+        self.offset, self.num_arenas, self.strong = lo, hi - lo, True
+
+    def processed(self, world):
+        """Arenas all ranks step per env step: every rank's own copy (weak), or the one set (strong)."""
+        return self.global_arenas if self.strong else self.num_arenas * world
 
     def name(self):
         t = self.tick_skip
@@ -162,7 +175,8 @@ class Workload:
 
     def config(self):
         ts = "1v1/2v2/3v3 (1:1:1)" if self.mixed else f"{self.team_size}v{self.team_size}"
-        return {"workload": self.name(), "preset": self.preset, "arenas": self.num_arenas, "teams": ts,
+        shard = {"arenas_this_rank": self.num_arenas, "first_arena": self.offset} if self.strong else {}
+        return {"workload": self.name(), "preset": self.preset, "arenas": self.global_arenas, **shard, "teams": ts,
                 "tick_skip": self.tick_skip, "narrowphase": "exact-bvh", "state": "fp32",
                 "actions": ("boost and jump each pressed with p=0.6" if self.bias else
                             "uniform over the 90-action table") + ", new each env step",
@@ -170,6 +184,19 @@ class Workload:
                 "rewards": "Goal, TouchBall, VelocityBallToGoal, VelocityPlayerToBall",
                 "terminals": f"goal or {EPISODE_TICKS} ticks; finished arenas reset on the device",
                 "graph": self.graph, "l2": "flushed between timed steps (256 MB write)"}
+
+
+def shard_range(team_sizes, num_arenas, rank, world):
+    """Rank `rank`'s contiguous arena range [lo, hi) of `num_arenas` arenas split over `world`
+    ranks with about the same number of cars each (team_sizes None: every arena the same size,
+    so the same number of arenas each).  Arenas are independent, so a split needs no exchange."""
+    if team_sizes is None:
+        cuts = [num_arenas * r // world for r in range(world + 1)]
+    else:
+        cum = np.concatenate([[0], np.cumsum(2 * np.asarray(team_sizes, np.int64))])
+        cuts = [int(np.searchsorted(cum, cum[-1] * r / world, side="left")) for r in range(world)] + [num_arenas]
+        cuts = [min(max(c, 0), num_arenas) for c in cuts]
+    return cuts[rank], cuts[rank + 1]
 
 
 class DevArray:
@@ -215,6 +242,8 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     wl = Workload(args)
+    if getattr(args, "strong", False):
+        wl.shard(rank, world)
     rewards = rsb.default_rewards(pkg.engine_library(), episode_max_ticks=EPISODE_TICKS)
     batch = rsb.Batch(pkg.engine_library(), wl.num_arenas, team_size=wl.team_size or None,
                       team_sizes=wl.team_sizes(), meshes_path=pkg.MESHES_DIR, device=dev, seed=0x5EED0000 + rank,
@@ -295,7 +324,7 @@ def run_ours(args, rank, world, dist):
         clocks_out.append(clocks.summary())
         s1 = batch.stats()
         total_ms = reduce_max(float(sum(times)), dist, dev)
-        value = wl.num_arenas * wl.tick_skip * steps * world / (total_ms / 1e3)
+        value = wl.processed(world) * wl.tick_skip * steps / (total_ms / 1e3)
         delta = {k: s1[k] - s0[k] for k in ("narrowphase_queries", "culled_queries", "missed_contacts", "solver_rows")}
         return value, total_ms, step_times, delta
 
@@ -402,7 +431,7 @@ def run_ours(args, rank, world, dist):
         e2e_times.append(time.perf_counter() - t0)
         h2d.append(4 * batch.num_cars + 4 * done.size)
         d2h.append(out_bytes)
-    e2e_value = wl.num_arenas * wl.tick_skip * world / reduce_max(statistics.median(e2e_times), dist, dev)
+    e2e_value = wl.processed(world) * wl.tick_skip / reduce_max(statistics.median(e2e_times), dist, dev)
 
     # state ring: a device capture (slot copies in HBM) and a restore, against the reference's
     # capture path (synchronise, download every car, ball and pad state)
@@ -522,8 +551,8 @@ def run_ours(args, rank, world, dist):
     res = {
         "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": total_ms / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random states)",
-        "config": cfg,
+        "scaling": "strong" if wl.strong else "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random states)", "config": cfg,
         "roofline": {"bound": "hbm", "kernel": "stepKernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "traffic_source": "ncu dram bytes of a settled 3v3 x 8192 launch, scaled by arenas"
@@ -1000,6 +1029,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--strong", action="store_true",
+                    help="split the preset's arenas over the ranks (balanced by car count) instead of one copy per rank")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

@@ -1869,7 +1869,8 @@ rsb_status rsb_build_vanta_obs(rsb_handle* h, void* stream) {
     vantaArenaKernel<<<(h->N + 127) / 128, 128, 0, st>>>(E, V, h->vantaTables);
     RSB_CUDA(cudaGetLastError());
     if (h->numCars > 0) {
-        vantaRowKernel<<<(h->numCars + 127) / 128, 128, 0, st>>>(E, V, h->vantaTables, h->numCars);
+        vantaRowKernel<<<(h->numCars + VANTA_THREADS - 1) / VANTA_THREADS, VANTA_THREADS, 0, st>>>(
+            E, V, h->vantaTables, h->numCars);
         RSB_CUDA(cudaGetLastError());
     }
     return RSB_OK;

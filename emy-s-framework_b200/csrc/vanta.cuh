@@ -14,8 +14,9 @@
 // (RocketSimCudaObs.cuh:70-186):
 //   vantaArenaKernel .. one thread per arena: pad availability and timers, demo timers, and
 //                       each player's coyote timers (once per arena tick);
-//   vantaRowKernel .... one thread per player: the row, written in place into the packed
-//                       [num_cars][366] buffer (rows in creation-slot order).
+//   vantaRowKernel .... one thread per player: the row, staged a section at a time in shared
+//                       memory and written by the warp into the packed [num_cars][366]
+//                       buffer (rows in creation-slot order).
 #pragma once
 #include "env_kernels.cuh"
 
@@ -351,11 +352,36 @@ RSB_D void vantaCarPacket(const EnvView& E, const VantaView& V, const VantaTable
     *o++ = dens;
 }
 
+// Writes the warp's 32 staged row sections (columns [c0, c0 + len) of rows row0 .. row0 + 31)
+// to the output, one row at a time with the lanes on consecutive columns: coalesced stores
+// instead of 32 rows 1,464 bytes apart per store instruction.
+constexpr int VANTA_THREADS = 128, VANTA_STAGE = 81;  // the longest section (ego)
+RSB_D void vantaFlush(float (*buf)[VANTA_STAGE], float* rows, int row0, int numCars, int c0, int len, int lane) {
+    __syncwarp();
+    for (int j = 0; j < 32 && row0 + j < numCars; j++) {
+        float* dst = rows + (size_t)(row0 + j) * VANTA_ROW + c0;
+        for (int k = lane; k < len; k += 32) dst[k] = buf[j][k];
+    }
+    __syncwarp();
+}
+
 // One thread per player (packed row r = carOffset[a] + slot): VantaObs::BuildObs
-// (VantaObsGpu.cuh:342-748) on the state after the arena update.
-__global__ void vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCars) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= numCars) return;
+// (VantaObsGpu.cuh:342-748) on the state after the arena update.  Each lane builds its row a
+// section at a time in its warp's shared-memory stage (odd row stride: no bank conflicts), and
+// the warp writes the section out with vantaFlush.  Lanes past the last row compute the last
+// row again (so that every lane reaches every flush) and write nothing.
+__global__ void __launch_bounds__(VANTA_THREADS) vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCars) {
+    __shared__ float stage[VANTA_THREADS / 32][32][VANTA_STAGE];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int row0 = blockIdx.x * blockDim.x + warp * 32;
+    const int r = min(row0 + lane, numCars - 1);
+    float(*buf)[VANTA_STAGE] = stage[warp];
+    float* const mine = buf[lane];
+    float* o = mine;
+    auto flush = [&](int c0) {
+        vantaFlush(buf, V.rows, row0, numCars, c0, (int)(o - mine), lane);
+        o = mine;
+    };
     const int N = E.N;
     // the arena of row r: the last arena whose first row is <= r
     int lo = 0, hi = N - 1;
@@ -365,7 +391,6 @@ __global__ void vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCar
         else hi = mid - 1;
     }
     const int a = lo, s = r - E.carOffset[a], M = 2 * E.teamSize[a];
-    float* o = V.rows + (size_t)r * VANTA_ROW;
 
     const uint32_t pf = carW(E, a, s, CW_FLAGS);
     const VBody world = carBody(E, a, s);
@@ -498,6 +523,8 @@ __global__ void vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCar
         *o++ = dens;
     }
 
+    flush(0);
+
     // ---- ball (29)
     *o++ = ball.pos.x / VA_POS_STD; *o++ = ball.pos.y / VA_POS_STD; *o++ = ball.pos.z / VA_POS_STD;
     *o++ = ball.vel.x / VA_BALL_VEL_STD; *o++ = ball.vel.y / VA_BALL_VEL_STD; *o++ = ball.vel.z / VA_BALL_VEL_STD;
@@ -518,6 +545,8 @@ __global__ void vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCar
             for (int j = 0; j < 6; j++) *o++ = 0.f;
         }
     }
+
+    flush(81);
 
     // ---- goal context (16)
     {
@@ -560,6 +589,8 @@ __global__ void vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCar
         *o++ = (ball.pos.y < 0.f) ? 1.f : 0.f;
     }
 
+    flush(110);  // goal and team context
+
     // ---- teammates and opponents by canonical distance to the ball (stable on ties)
     int mate[MAX_CARS], opp[MAX_CARS];
     float mateD[MAX_CARS], oppD[MAX_CARS];
@@ -586,11 +617,13 @@ __global__ void vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCar
     for (int i = 0; i < 2; i++) {
         if (i < nm) vantaCarPacket(E, V, T, a, mate[i], self, ball.pos, inv, mirror, av0, av1, o);
         else for (int k = 0; k < 39; k++) *o++ = 0.f;
+        flush(132 + 39 * i);
     }
     const int oppLimit = V.onlyClosestOpp ? 1 : 3;
     for (int i = 0; i < 3; i++) {
         if (i < oppLimit && i < no) vantaCarPacket(E, V, T, a, opp[i], self, ball.pos, inv, mirror, av0, av1, o);
         else for (int k = 0; k < 39; k++) *o++ = 0.f;
+        flush(132 + 39 * (2 + i));
     }
     for (int i = 0; i < 2; i++) *o++ = i < nm ? 1.f : 0.f;
     for (int i = 0; i < 3; i++) *o++ = (i < oppLimit && i < no) ? 1.f : 0.f;
@@ -607,6 +640,7 @@ __global__ void vantaRowKernel(EnvView E, VantaView V, VantaTables T, int numCar
             *o++ = 1.f / (1.f + __uint_as_float(vaW(V, N, a, VA_TIMER + idx)) / tMax);
         }
     }
+    flush(327);  // validity mask and pads
 }
 
 }  // namespace rsb

@@ -1,8 +1,8 @@
 """The CUDA engine against the committed golden rollouts of the reference CPU RocketSim
 (tests/golden/soccar_trajectories.npz): the same states and actions, 120 free-running ticks.
-Discrete car flags must match on at least 99.9% of car-ticks and positions stay within the
-free-running drift bounds of the trajectory tests; arenas whose recorded car order is not
-reverse creation order are left out."""
+Discrete car flags and car and ball positions must equal the recorded ones at every tick;
+arenas whose recorded car order is not reverse creation order are left out (the reference's
+car set is hashed by heap address)."""
 from __future__ import annotations
 
 import os
@@ -14,8 +14,6 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DRIFT_MEDIAN_UU = 0.05
-DRIFT_P99_UU = 25.0
 
 
 def test_engine_follows_golden(pkg, meshes_dir):
@@ -34,8 +32,10 @@ def test_engine_follows_golden(pkg, meshes_dir):
     reverse = np.array([np.array_equal(order[a, :2 * t], np.arange(2 * t)[::-1]) for a, t in enumerate(ts)])
     keep = np.repeat(reverse, 2 * ts)
     flag_ok = (car_flags[:, keep] == g["car_flags"][:, keep]).mean()
-    assert flag_ok >= 0.999, flag_ok
-    drift = np.linalg.norm(car_kin[:, keep, 0] - g["car_kin"][:, keep, 0], axis=-1)
-    assert np.median(drift) <= DRIFT_MEDIAN_UU and np.percentile(drift, 99) <= DRIFT_P99_UU
+    drift_all = np.linalg.norm(car_kin[:, keep, 0] - g["car_kin"][:, keep, 0], axis=-1)
+    print(f"GOLDEN flags equal {flag_ok:.6f}; car drift max {drift_all.max():.4g} uu, cars with any drift "
+          f"{int((drift_all.max(axis=0) > 0).sum())} of {int(keep.sum())}")
+    assert flag_ok == 1.0, flag_ok
+    assert drift_all.max() == 0, float(drift_all.max())
     bdrift = np.linalg.norm(ball_kin[:, reverse, 0] - g["ball_kin"][:, reverse, 0], axis=-1)
-    assert np.median(bdrift) <= DRIFT_MEDIAN_UU and np.percentile(bdrift, 99) <= DRIFT_P99_UU
+    assert bdrift.max() == 0, float(bdrift.max())

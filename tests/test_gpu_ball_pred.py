@@ -46,8 +46,8 @@ def test_prediction_matches_oracle(pkg, oracle_lib, meshes_dir):
         d = np.linalg.norm(vec(pe[:, k], "pos") - vec(po[:, k], "pos"), axis=1)
         same = (pe[:, k].tobytes() == po[:, k].tobytes())
         print(f"PRED tick {t}: identical={int((d == 0).sum())}/{n} max_pos_diff={d.max():.3g} uu over1uu={int((d > 1).sum())} all_bytes_equal={same}")
-        # measured on B200: at most 0.004 uu after 360 ticks (one-ulp differences through bounces)
-        assert d.max() <= 0.05, f"tick {t}: a ball {d.max():.3g} uu from the oracle"
+        # the device's arithmetic is the reference's: every slice equal byte for byte
+        assert same, f"tick {t}: {int((d != 0).sum())} balls differ, the largest by {d.max():.3g} uu"
 
 
 def test_repeated_predictions_match_oracle(pkg, oracle_lib, meshes_dir):

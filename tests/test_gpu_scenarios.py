@@ -245,6 +245,10 @@ def test_reference_scenario(pkg, oracle_lib, meshes_dir, name):
     print(f"SCENARIO {name} " + " ".join(f"{k}={v:.3g}" for k, v in got.items()))
     for (k, v), limit in zip(got.items(), tol):
         assert v <= limit, f"{name}: {k} differs by {v:.4g} (tolerance {limit}); {got}"
+    # beyond the reference's own tolerances: positions, velocities and boost are equal
+    # (the heading metric keeps a float64 arccos residue of ~1e-6 degrees on equal vectors)
+    for k in ("ball_pos", "ball_vel", "car_pos", "car_vel", "boost"):
+        assert got[k] == 0, f"{name}: {k} differs by {got[k]:.4g}; {got}"
     assert np.array_equal(ce["is_on_ground"], co["is_on_ground"]), f"{name}: on-ground flags differ"
     assert np.array_equal(ce["is_demoed"], co["is_demoed"]), f"{name}: demo flags differ"
     assert ie["goal_scored"] == io["goal_scored"] and ie["goal_team"] == io["goal_team"], f"{name}: goal differs"

@@ -28,6 +28,8 @@ def test_ball_trajectories_match_oracle_120_ticks(pkg, oracle_lib, meshes_dir):
         assert max_excess(vec(a, "pos"), vec(b, "pos"), POS_ABS_UU) <= 0, f"tick {tick} position"
         assert max_excess(vec(a, "vel"), vec(b, "vel"), VEL_ABS_UU) <= 0, f"tick {tick} velocity"
         assert max_excess(vec(a, "ang_vel"), vec(b, "ang_vel"), 1e-4) <= 0, f"tick {tick} angular velocity"
+        # and, free-running, byte for byte
+        assert a.tobytes() == b.tobytes(), f"tick {tick}: ball states differ"
 
 
 def test_multi_tick_launch_is_bit_identical(pkg, meshes_dir):
@@ -87,5 +89,5 @@ def test_floor_bounce_invariants_and_oracle(pkg, oracle_lib, meshes_dir):
     be = bounce_invariants(eng)
     bo = bounce_invariants(ora)
     assert be[0] and be[1] >= 0.5 * 91.25 and be[2] <= be[3] * 1.001, be
-    assert abs(be[1] - bo[1]) < 1e-3 and abs(be[2] - bo[2]) <= 1e-4 * bo[2]
-    assert np.allclose(vec(eng.get_balls(), "pos"), vec(ora.get_balls(), "pos"), atol=1e-2)
+    assert be[1] == bo[1] and be[2] == bo[2], (be, bo)
+    assert eng.get_balls().tobytes() == ora.get_balls().tobytes()
